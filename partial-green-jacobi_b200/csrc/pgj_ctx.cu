@@ -1,0 +1,392 @@
+// libpgj context, workspace layout, certified solve and the C ABI entry points.
+//
+// The certified solve follows Resident._solve_batch (exp/asg_gpu_resident_20261103/resident.py:186-209):
+// rhs and targets; certify (u <- P u, r = f - K u, ||r||); then up to three attempts of
+// [initialise masks and directions; iterate while any load is active; certify], restarting only
+// when a certificate fails and no latch forbids it. Each attempt is one CUDA graph: the iteration
+// loop is a device-side WHILE conditional node whose condition the last kernel of every iteration
+// sets from the per-load masks, so the host only synchronises once per attempt to read the
+// certificate (the reference polls active.any() every 4 iterations).
+#include "pgj_internal.h"
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+namespace pgj {
+
+static thread_local int g_last_cuda_error = 0;
+int set_cuda_error(cudaError_t e) {
+  g_last_cuda_error = int(e);
+  return PGJ_ERR_LAUNCH;
+}
+
+struct Graphs {
+  cudaStream_t cap = nullptr;  // private capture stream
+  int loads = 0;
+  cudaGraphExec_t cert = nullptr;
+  cudaGraphExec_t attempt = nullptr;
+  ~Graphs() {
+    if (cert) cudaGraphExecDestroy(cert);
+    if (attempt) cudaGraphExecDestroy(attempt);
+    if (cap) cudaStreamDestroy(cap);
+  }
+};
+
+static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+static Layout make_layout(int n, int L, int prec) {
+  Layout y;
+  const size_t N = size_t(n) * n * n, N3 = 3 * N;
+  const size_t ns = size_t(n / 2 + 1), Nh = size_t(n) * n * ns;
+  const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t at = o; o = align_up(o + bytes, 256); return at; };
+  y.scal = take(sizeof(LoadScalars) * size_t(2 * L));
+  y.macros = take(sizeof(double) * 6 * size_t(L));
+  y.cond = take(64);
+  y.aux = take(sizeof(double) * kAuxDoubles);
+  y.tw = take(size_t(n) * (sizeof(double2) + sizeof(float2)));
+  const size_t pslots = size_t(4 * L > 24 ? 4 * L : 24);
+  y.partials = take(sizeof(double) * pslots * kMaxPartials);
+  y.a = take(sizeof(double) * N);
+  y.scale = take(sizeof(double) * N3);
+  y.symbol = take(sizeof(double) * 6 * Nh);
+  y.symbol32 = take(prec == PGJ_FP32 ? sizeof(float) * 6 * Nh : 0);
+  y.solutions = take(sizeof(double) * N3 * L);
+  y.f = take(sizeof(double) * N3 * L);
+  y.x = take(sizeof(double) * N3 * L);
+  y.r64 = take(prec == PGJ_FP32 ? sizeof(double) * N3 * L : 0);
+  y.r = take(tsz * N3 * L);
+  y.p = take(tsz * N3 * L);
+  y.q = take(tsz * N3 * L);
+  y.sw = take(tsz * N3 * L);
+  y.spec = take(2 * tsz * 3 * Nh * L);
+  y.total = o;
+  return y;
+}
+
+// ------------------------------------------------------------------------------------ graphs
+static int capture_cert(pgj_ctx* c, int L, cudaStream_t s) {
+  int st = launch_project_u(c, L, c->x, s);
+  if (st) return st;
+  return launch_stencil(c, kResidual, L, PGJ_FP64, c->x, c->r, c->f, nullptr, s);
+}
+
+static int capture_iteration(pgj_ctx* c, int L, cudaStream_t s, cudaGraphConditionalHandle h, bool last) {
+  int st;
+  if ((st = launch_stencil(c, kPCG, L, PGJ_FP64, c->p, c->q, nullptr, nullptr, s))) return st;
+  if ((st = launch_update_ur(c, L, PGJ_FP64, c->x, nullptr, s))) return st;
+  if ((st = launch_green(c, L, PGJ_FP64, c->r, false, s))) return st;
+  return launch_update_p(c, L, PGJ_FP64, false, s, h, last);
+}
+
+static int end_capture(cudaStream_t s, cudaGraph_t* g, int st) {
+  cudaError_t e = cudaStreamEndCapture(s, g);
+  if (st) { if (*g) cudaGraphDestroy(*g); *g = nullptr; return st; }
+  if (e != cudaSuccess) return set_cuda_error(e);
+  return PGJ_OK;
+}
+
+static int build_graphs(pgj_ctx* c, int L) {
+  Graphs* G = c->graphs;
+  if (G->loads == L && G->cert && G->attempt) return PGJ_OK;
+  if (G->cert) { cudaGraphExecDestroy(G->cert); G->cert = nullptr; }
+  if (G->attempt) { cudaGraphExecDestroy(G->attempt); G->attempt = nullptr; }
+  cudaStream_t s = G->cap;
+  cudaGraph_t g = nullptr;
+  int st;
+  cudaError_t e;
+  // certification graph
+  if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return set_cuda_error(e);
+  st = capture_cert(c, L, s);
+  if ((st = end_capture(s, &g, st))) return st;
+  e = cudaGraphInstantiate(&G->cert, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  // attempt graph: init -> while(any active){iteration} -> certify
+  if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return set_cuda_error(e);
+  st = launch_init_mask(c, L, s);
+  if (!st) st = launch_green(c, L, PGJ_FP64, c->r, true, s);
+  if (!st) st = launch_update_p(c, L, PGJ_FP64, true, s, 0, false);
+  cudaGraphNode_t node = nullptr;
+  if (!st) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t cg = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &ndeps);
+    cudaGraphConditionalHandle h = 0;
+    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, cg, deps, ndeps, &cp);
+    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) {
+      st = set_cuda_error(e);
+    } else {
+      cudaGraph_t body = cp.conditional.phGraph_out[0];
+      cudaStream_t s2;
+      e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+      if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+      if (e != cudaSuccess) {
+        st = set_cuda_error(e);
+      } else {
+        st = capture_iteration(c, L, s2, h, true);
+        cudaGraph_t bg = body;
+        cudaError_t e2 = cudaStreamEndCapture(s2, &bg);
+        if (!st && e2 != cudaSuccess) st = set_cuda_error(e2);
+      }
+      cudaStreamDestroy(s2);
+    }
+  }
+  if (!st) st = capture_cert(c, L, s);
+  if ((st = end_capture(s, &g, st))) return st;
+  e = cudaGraphInstantiate(&G->attempt, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  G->loads = L;
+  return PGJ_OK;
+}
+
+}  // namespace pgj
+
+using namespace pgj;
+
+extern "C" {
+
+int pgj_version(void) { return 1; }
+
+const char* pgj_status_string(int status) {
+  switch (status) {
+    case PGJ_OK: return "ok";
+    case PGJ_ERR_ARGUMENT: return "invalid argument (pointer, size, shape or value)";
+    case PGJ_ERR_UNSUPPORTED: return "unsupported grid size (FFT radices 2,3,5, even n, 4 <= n <= 256)";
+    case PGJ_ERR_LAUNCH: return "CUDA launch or runtime error";
+    case PGJ_ERR_NONFINITE: return "non-finite value or non-positive curvature";
+    case PGJ_ERR_ITERATION_CAP: return "iteration cap reached without certification";
+    case PGJ_ERR_CERTIFICATION: return "true residual certification failed";
+    case PGJ_ERR_TIMEOUT: return "bounded device wait expired";
+    case PGJ_ERR_WORKSPACE: return "workspace missing, too small or misaligned";
+    default: return "unknown status";
+  }
+}
+
+int pgj_last_cuda_error(void) { return g_last_cuda_error; }
+
+static bool grid_ok(int n) {
+  FFTPlan p;
+  return n >= 4 && n <= 256 && make_fft_plan(n, &p);
+}
+
+int pgj_workspace_bytes(int n, int loads, int precision, size_t* bytes) {
+  if (!bytes || loads < 1 || loads > kMaxLoads || (precision != PGJ_FP64 && precision != PGJ_FP32))
+    return PGJ_ERR_ARGUMENT;
+  if (!grid_ok(n)) return PGJ_ERR_UNSUPPORTED;
+  *bytes = make_layout(n, loads, precision).total;
+  return PGJ_OK;
+}
+
+int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void* workspace, size_t workspace_bytes,
+                   void* stream, pgj_ctx** out) {
+  if (!out || loads < 1 || loads > kMaxLoads || !(mu > 0) || !(lam + 2 * mu / 3 > 0) ||
+      (precision != PGJ_FP64 && precision != PGJ_FP32))
+    return PGJ_ERR_ARGUMENT;
+  if (!grid_ok(n)) return PGJ_ERR_UNSUPPORTED;
+  Layout y = make_layout(n, loads, precision);
+  if (!workspace || workspace_bytes < y.total || (reinterpret_cast<uintptr_t>(workspace) & 255)) return PGJ_ERR_WORKSPACE;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  pgj_ctx* c = new (std::nothrow) pgj_ctx();
+  if (!c) return PGJ_ERR_ARGUMENT;
+  c->n = n; c->L = loads; c->prec = precision; c->lam = lam; c->mu = mu;
+  c->N = (long long)n * n * n; c->ns = n / 2 + 1; c->Nh = (long long)n * n * c->ns;
+  c->kc = make_opconst(n, lam, mu);
+  make_fft_plan(n, &c->plan);
+  c->sg = stencil_geom(n, loads);
+  c->fg = fft_geom(n, precision == PGJ_FP32 ? 4 : 8);
+  c->lay = y;
+  c->base = static_cast<char*>(workspace);
+  c->bytes = workspace_bytes;
+  char* b = c->base;
+  c->a = reinterpret_cast<double*>(b + y.a);
+  c->scale = reinterpret_cast<double*>(b + y.scale);
+  c->symbol = reinterpret_cast<double*>(b + y.symbol);
+  c->symbol32 = precision == PGJ_FP32 ? reinterpret_cast<float*>(b + y.symbol32) : nullptr;
+  c->tw = b + y.tw;
+  c->solutions = reinterpret_cast<double*>(b + y.solutions);
+  c->f = reinterpret_cast<double*>(b + y.f);
+  c->x = reinterpret_cast<double*>(b + y.x);
+  c->r64 = precision == PGJ_FP32 ? reinterpret_cast<double*>(b + y.r64) : nullptr;
+  c->r = b + y.r; c->p = b + y.p; c->q = b + y.q; c->sw = b + y.sw; c->spec = b + y.spec;
+  c->partials = reinterpret_cast<double*>(b + y.partials);
+  c->scal = reinterpret_cast<LoadScalars*>(b + y.scal);
+  c->macros = reinterpret_cast<double*>(b + y.macros);
+  c->cond = reinterpret_cast<int*>(b + y.cond);
+  c->aux = reinterpret_cast<double*>(b + y.aux);
+  c->alpha = 0.0;
+  c->inner_rtol = 1e-5;
+  c->last_refinements = 0;
+  c->graphs = new (std::nothrow) Graphs();
+  int st = PGJ_OK;
+  cudaError_t e = cudaMemsetAsync(workspace, 0, y.total, s);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->graphs->cap, cudaStreamNonBlocking);
+  if (e != cudaSuccess) st = set_cuda_error(e);
+  if (!st) st = prepare_stencil_kernels();
+  if (!st) st = prepare_fft_kernels();
+  if (!st) st = init_fft_tables(c, s);
+  if (!st) st = build_symbol(n, lam, mu, c->symbol, c->symbol32, s);
+  if (!st) {
+    // unit Voigt macros for the homogenized tensor
+    double eye[36] = {0};
+    for (int i = 0; i < 6; ++i) eye[i * 6 + i] = 1.0;
+    e = cudaMemcpyAsync(c->aux + kAuxVoigt, eye, sizeof(eye), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) st = set_cuda_error(e);
+  }
+  if (!st) st = launch_scale(c, 0.0, s);  // scale = 1 until an alpha is selected
+  if (st) {
+    delete c->graphs;
+    delete c;
+    return st;
+  }
+  *out = c;
+  return PGJ_OK;
+}
+
+int pgj_ctx_destroy(pgj_ctx* ctx) {
+  if (!ctx) return PGJ_ERR_ARGUMENT;
+  delete ctx->graphs;
+  delete ctx;
+  return PGJ_OK;
+}
+
+double* pgj_ctx_solutions(pgj_ctx* ctx) { return ctx ? ctx->solutions : nullptr; }
+double* pgj_ctx_scale(pgj_ctx* ctx) { return ctx ? ctx->scale : nullptr; }
+double* pgj_ctx_material(pgj_ctx* ctx) { return ctx ? ctx->a : nullptr; }
+
+int pgj_set_material(pgj_ctx* c, const double* a, void* stream) {
+  if (!c || !a) return PGJ_ERR_ARGUMENT;
+  cudaError_t e = cudaMemcpyAsync(c->a, a, sizeof(double) * size_t(c->N), cudaMemcpyDeviceToDevice,
+                                  static_cast<cudaStream_t>(stream));
+  return e == cudaSuccess ? PGJ_OK : set_cuda_error(e);
+}
+
+int pgj_set_alpha(pgj_ctx* c, double alpha, void* stream) {
+  if (!c || !std::isfinite(alpha)) return PGJ_ERR_ARGUMENT;
+  c->alpha = alpha;
+  return launch_scale(c, alpha, static_cast<cudaStream_t>(stream));
+}
+
+int pgj_apply(pgj_ctx* c, int loads, const double* p, const int32_t* active, double* q, void* stream) {
+  if (!c || !p || !q || loads < 1 || loads > c->L) return PGJ_ERR_ARGUMENT;
+  return launch_stencil(c, kPlain, loads, PGJ_FP64, p, q, nullptr, active, static_cast<cudaStream_t>(stream));
+}
+
+int pgj_apply_f32(pgj_ctx* c, int loads, const float* p, const int32_t* active, float* q, void* stream) {
+  if (!c || !p || !q || loads < 1 || loads > c->L) return PGJ_ERR_ARGUMENT;
+  return launch_stencil(c, kPlain, loads, PGJ_FP32, p, q, nullptr, active, static_cast<cudaStream_t>(stream));
+}
+
+static int stage_macros(pgj_ctx* c, int loads, const double* macros, cudaStream_t s) {
+  for (int i = 0; i < 6 * loads; ++i)
+    if (!std::isfinite(macros[i])) return PGJ_ERR_NONFINITE;
+  cudaError_t e = cudaMemcpyAsync(c->macros, macros, sizeof(double) * 6 * size_t(loads), cudaMemcpyHostToDevice, s);
+  return e == cudaSuccess ? PGJ_OK : set_cuda_error(e);
+}
+
+int pgj_rhs(pgj_ctx* c, int loads, const double* macros, double* f, void* stream) {
+  if (!c || !macros || !f || loads < 1 || loads > c->L) return PGJ_ERR_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int st = stage_macros(c, loads, macros, s);
+  if (st) return st;
+  return launch_rhs(c, loads, c->macros, f, s);
+}
+
+int pgj_precondition(pgj_ctx* c, int loads, const double* r, double* z, void* stream) {
+  if (!c || !r || !z || loads < 1 || loads > c->L || c->prec != PGJ_FP64) return PGJ_ERR_ARGUMENT;
+  return launch_green_standalone(c, loads, r, z, static_cast<cudaStream_t>(stream));
+}
+
+int pgj_green_symbol(int n, double lam, double mu, double* symbol, void* stream) {
+  if (!symbol || !(mu > 0)) return PGJ_ERR_ARGUMENT;
+  if (!grid_ok(n)) return PGJ_ERR_UNSUPPORTED;
+  return build_symbol(n, lam, mu, symbol, nullptr, static_cast<cudaStream_t>(stream));
+}
+
+int pgj_set_inner_rtol(pgj_ctx* c, double inner_rtol) {
+  if (!c || !(inner_rtol > 0 && inner_rtol < 1)) return PGJ_ERR_ARGUMENT;
+  c->inner_rtol = inner_rtol;
+  return PGJ_OK;
+}
+
+int pgj_last_refinements(pgj_ctx* c) { return c ? c->last_refinements : -1; }
+
+int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* u, pgj_load_info* info, void* stream) {
+  if (!c || !macros || !u || !info || loads < 1 || loads > c->L || !(rtol > 0)) return PGJ_ERR_ARGUMENT;
+  if (c->prec != PGJ_FP64) return PGJ_ERR_UNSUPPORTED;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t N3 = 3 * size_t(c->N);
+  int st = stage_macros(c, loads, macros, s);
+  if (!st) st = launch_rhs(c, loads, c->macros, c->f, s);
+  if (!st) st = launch_norms(c, loads, c->f, rtol, s);
+  if (st) return st;
+  cudaError_t e = cudaSuccess;
+  if (u != c->x) e = cudaMemcpyAsync(c->x, u, sizeof(double) * N3 * loads, cudaMemcpyDeviceToDevice, s);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  if ((st = build_graphs(c, loads))) return st;
+  if ((e = cudaGraphLaunch(c->graphs->cert, s)) != cudaSuccess) return set_cuda_error(e);
+  std::vector<LoadScalars> h(loads);
+  std::vector<int> ok(loads, 0);
+  int restarts = 0;
+  for (;;) {
+    if ((e = cudaGraphLaunch(c->graphs->attempt, s)) != cudaSuccess) return set_cuda_error(e);
+    e = cudaMemcpyAsync(h.data(), c->scal, sizeof(LoadScalars) * loads, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    bool all = true, anybad = false, capped = false;
+    for (int l = 0; l < loads; ++l) {
+      const double thr = std::sqrt(h[l].target2);
+      ok[l] = std::isfinite(h[l].absolute) && h[l].absolute <= thr && h[l].bad == 0;
+      all = all && ok[l];
+      anybad = anybad || h[l].bad;
+      capped = capped || (!ok[l] && h[l].iterations >= 4000);
+    }
+    if (all || restarts >= 2 || anybad || capped) break;
+    ++restarts;
+  }
+  if (u != c->x) e = cudaMemcpyAsync(u, c->x, sizeof(double) * N3 * loads, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  bool all = true;
+  for (int l = 0; l < loads; ++l) {
+    pgj_load_info& I = info[l];
+    I.rhs_norm = h[l].norm;
+    I.absolute_residual = h[l].absolute;
+    I.threshold = std::sqrt(h[l].target2);
+    I.relative_residual = h[l].absolute / (h[l].norm > 1e-300 ? h[l].norm : 1e-300);
+    I.iterations = h[l].iterations;
+    I.converged = ok[l];
+    I.restarts = restarts;
+    I.bad = h[l].bad;
+    all = all && ok[l];
+  }
+  c->last_refinements = 1;
+  return all ? PGJ_OK : PGJ_ERR_CERTIFICATION;
+}
+
+int pgj_energies(pgj_ctx* c, int loads, const double* u, const double* macros, double* e, void* stream) {
+  if (!c || !u || !macros || !e || loads < 1 || loads > kMaxLoads || loads > c->L) return PGJ_ERR_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  int st = stage_macros(c, loads, macros, s);
+  if (st) return st;
+  return launch_energies(c, loads, u, c->macros, e, s);
+}
+
+int pgj_effective_tensor(pgj_ctx* c, const double* u, double* C, void* stream) {
+  if (!c || !u || !C) return PGJ_ERR_ARGUMENT;
+  return launch_effective_tensor(c, u, C, nullptr, static_cast<cudaStream_t>(stream));
+}
+
+}  // extern "C"

@@ -1,0 +1,607 @@
+// Green apply z = P(s . G(s . P r)) with hand-written shared-memory FFTs.
+//
+// G is the FI HEX8 Green operator of the homogeneous medium C0 on the periodic grid: a real
+// 3D DFT of each displacement component, multiplication by the real symmetric 3x3 Fourier symbol
+// (6 coefficients per half-spectrum point, 1/N folded in), and the unnormalised inverse DFT
+// (the reference uses cuFFT via torch.fft.rfftn/irfftn: exp/asg_gpu_resident_20261103/resident.py:109-117,
+// spectral_three in scalar_fi.cu:38-44). Here the transform is five passes over the half
+// spectrum, each a batch of 1D FFTs in shared memory (Stockham autosort, radices 2,3,4,5,8):
+//   FX : v = s.(r - mean r) per row, two real rows packed into one complex FFT, R2C split.
+//   FY : complex FFT along y.
+//   FZ : complex FFT along z, symbol multiply, the Parseval form <v, G v> (= r.z), inverse along z.
+//   IFY: inverse along y.
+//   IFX: C2R along x (two rows per complex FFT), s.w and its per-component sums (projection P).
+// Loads whose recurrence is inactive are skipped block-uniformly.
+#include "pgj_internal.h"
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+namespace pgj {
+
+bool make_fft_plan(int n, FFTPlan* plan) {
+  plan->n = n;
+  plan->nst = 0;
+  int m = n;
+  while (m % 8 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 8; m /= 8; }
+  while (m % 4 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 4; m /= 4; }
+  while (m % 2 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 2; m /= 2; }
+  while (m % 3 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 3; m /= 3; }
+  while (m % 5 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 5; m /= 5; }
+  return m == 1 && n % 2 == 0 && n >= 4;
+}
+
+// smem budget per block for the line buffers (two ping-pong buffers)
+static constexpr size_t kFFTSmemBudget = 200 * 1024;
+
+FFTGeom fft_geom(int n, int elem_bytes) {
+  FFTGeom g;
+  const size_t cb = 2 * size_t(elem_bytes);  // complex bytes
+  const size_t line = size_t(n + 1) * cb;
+  const int ns = n / 2 + 1;
+  // x passes: rb rows -> 3 rb / 2 complex lines; keep <= ~48 lines and rb | n*n
+  int rb = 16;
+  while (rb > 2 && ((size_t(n) * n) % rb != 0 || 2 * (3 * size_t(rb) / 2) * line > kFFTSmemBudget)) rb /= 2;
+  g.rb = rb;
+  // y passes: kcy kx columns per block
+  int kcy = ns;
+  while (kcy > 1 && 2 * size_t(kcy) * line > kFFTSmemBudget) kcy = (kcy + 1) / 2;
+  g.kcy = kcy;
+  g.nky = (ns + kcy - 1) / kcy;
+  int kcz = ns;
+  while (kcz > 1 && 2 * 3 * size_t(kcz) * line > kFFTSmemBudget) kcz = (kcz + 1) / 2;
+  // prefer an even split of ns
+  int nkz = (ns + kcz - 1) / kcz;
+  kcz = (ns + nkz - 1) / nkz;
+  g.kcz = kcz;
+  g.nkz = nkz;
+  return g;
+}
+
+// ----------------------------------------------------------------------------- radix kernels
+// Forward transforms use e^{-2 pi i jk/R}; inverse ones the conjugate (unnormalised).
+template <typename C>
+__device__ __forceinline__ void dft2(C& a, C& b) { C t = a; a = cadd(t, b); b = csub(t, b); }
+
+template <typename C>
+__device__ __forceinline__ void dft4(C& v0, C& v1, C& v2, C& v3, bool inv) {
+  C a = cadd(v0, v2), b = csub(v0, v2), c = cadd(v1, v3), d = cmul_mi(csub(v1, v3), inv);
+  v0 = cadd(a, c); v2 = csub(a, c); v1 = cadd(b, d); v3 = csub(b, d);
+}
+
+template <typename T, int R> struct Radix;
+
+template <typename T> struct Radix<T, 2> {
+  using C = cplx<T>;
+  static __device__ __forceinline__ void run(C (&v)[2], bool) { dft2(v[0], v[1]); }
+};
+template <typename T> struct Radix<T, 4> {
+  using C = cplx<T>;
+  static __device__ __forceinline__ void run(C (&v)[4], bool inv) { dft4(v[0], v[1], v[2], v[3], inv); }
+};
+template <typename T> struct Radix<T, 8> {
+  using C = cplx<T>;
+  static __device__ __forceinline__ void run(C (&v)[8], bool inv) {
+    const T r2 = T(0.70710678118654752440);
+    C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
+    C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
+    dft4(e0, e1, e2, e3, inv);
+    dft4(o0, o1, o2, o3, inv);
+    // twiddles W8^k (forward (1-i)/sqrt2 ...), conjugated for the inverse
+    C t1, t2, t3;
+    if (!inv) {
+      t1.x = r2 * (o1.x + o1.y); t1.y = r2 * (o1.y - o1.x);
+      t2.x = o2.y; t2.y = -o2.x;
+      t3.x = r2 * (o3.y - o3.x); t3.y = -r2 * (o3.x + o3.y);
+    } else {
+      t1.x = r2 * (o1.x - o1.y); t1.y = r2 * (o1.x + o1.y);
+      t2.x = -o2.y; t2.y = o2.x;
+      t3.x = -r2 * (o3.x + o3.y); t3.y = r2 * (o3.x - o3.y);
+    }
+    v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
+    v[1] = cadd(e1, t1); v[5] = csub(e1, t1);
+    v[2] = cadd(e2, t2); v[6] = csub(e2, t2);
+    v[3] = cadd(e3, t3); v[7] = csub(e3, t3);
+  }
+};
+template <typename T> struct Radix<T, 3> {
+  using C = cplx<T>;
+  static __device__ __forceinline__ void run(C (&v)[3], bool inv) {
+    const T s3 = T(0.86602540378443864676);
+    C s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
+    C t; t.x = v[0].x - T(0.5) * s.x; t.y = v[0].y - T(0.5) * s.y;
+    v[0] = cadd(v[0], s);
+    C u = cmul_mi(d, inv); u.x *= s3; u.y *= s3;
+    v[1] = cadd(t, u); v[2] = csub(t, u);
+  }
+};
+template <typename T> struct Radix<T, 5> {
+  using C = cplx<T>;
+  static __device__ __forceinline__ void run(C (&v)[5], bool inv) {
+    const T c1 = T(0.30901699437494742410), c2 = T(-0.80901699437494742410);
+    const T s1 = T(0.95105651629515357212), s2 = T(0.58778525229247312917);
+    C s14 = cadd(v[1], v[4]), d14 = csub(v[1], v[4]), s23 = cadd(v[2], v[3]), d23 = csub(v[2], v[3]);
+    C a1, a2, b1, b2;
+    a1.x = v[0].x + c1 * s14.x + c2 * s23.x; a1.y = v[0].y + c1 * s14.y + c2 * s23.y;
+    a2.x = v[0].x + c2 * s14.x + c1 * s23.x; a2.y = v[0].y + c2 * s14.y + c1 * s23.y;
+    b1.x = s1 * d14.x + s2 * d23.x; b1.y = s1 * d14.y + s2 * d23.y;
+    b2.x = s2 * d14.x - s1 * d23.x; b2.y = s2 * d14.y - s1 * d23.y;
+    v[0] = cadd(v[0], cadd(s14, s23));
+    C ib1 = cmul_mi(b1, inv), ib2 = cmul_mi(b2, inv);
+    v[1] = cadd(a1, ib1); v[4] = csub(a1, ib1);
+    v[2] = cadd(a2, ib2); v[3] = csub(a2, ib2);
+  }
+};
+
+// One Stockham stage over `nlines` lines of length n (pitch `pitch`): out[(j/Ns)Ns R + j%Ns + r Ns] =
+// DFT_R over r of in[j + r n/R] * W^{r (j%Ns)}, W = e^{-2 pi i/(Ns R)}.
+template <typename T, int R>
+__device__ __forceinline__ void stage(const cplx<T>* __restrict__ src, cplx<T>* __restrict__ dst, int nlines, int pitch,
+                                      int n, int Ns, const cplx<T>* __restrict__ tw, bool inv, int tid, int nthr) {
+  using C = cplx<T>;
+  const int nb = n / R;
+  const int total = nlines * nb;
+  const int step = n / (Ns * R);
+  for (int k = tid; k < total; k += nthr) {
+    const int line = k % nlines, j = k / nlines;
+    const C* s = src + line * pitch;
+    C* d = dst + line * pitch;
+    const int jm = j % Ns;
+    C v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[r] = s[j + r * nb];
+    if (jm) {
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        C w = tw[r * jm * step];
+        if (inv) w.y = -w.y;
+        v[r] = cmul(v[r], w);
+      }
+    }
+    Radix<T, R>::run(v, inv);
+    const int base = (j - jm) * R + jm;
+#pragma unroll
+    for (int r = 0; r < R; ++r) d[base + r * Ns] = v[r];
+  }
+}
+
+// Runs all stages; returns the buffer holding the result.
+template <typename T>
+__device__ cplx<T>* fft_lines(cplx<T>* b0, cplx<T>* b1, int nlines, int pitch, const FFTPlan& pl,
+                              const cplx<T>* tw, bool inv, int tid, int nthr) {
+  cplx<T>* src = b0;
+  cplx<T>* dst = b1;
+  int Ns = 1;
+  for (int st = 0; st < pl.nst; ++st) {
+    const int R = pl.radix[st];
+    switch (R) {
+      case 8: stage<T, 8>(src, dst, nlines, pitch, pl.n, Ns, tw, inv, tid, nthr); break;
+      case 4: stage<T, 4>(src, dst, nlines, pitch, pl.n, Ns, tw, inv, tid, nthr); break;
+      case 2: stage<T, 2>(src, dst, nlines, pitch, pl.n, Ns, tw, inv, tid, nthr); break;
+      case 3: stage<T, 3>(src, dst, nlines, pitch, pl.n, Ns, tw, inv, tid, nthr); break;
+      default: stage<T, 5>(src, dst, nlines, pitch, pl.n, Ns, tw, inv, tid, nthr); break;
+    }
+    __syncthreads();
+    cplx<T>* t = src; src = dst; dst = t;
+    Ns *= R;
+  }
+  return src;
+}
+
+struct GreenArgs {
+  int n, ns;
+  FFTPlan plan;
+  FFTGeom geo;
+  const void* r;         // (L,3N) T input residual
+  const double* scale;   // (3N) fp64 scale field
+  void* spec;            // (L,3,n,n,ns) complex T
+  const void* sym;       // (6,Nh) T symbol
+  const void* tw;        // n complex T twiddles (forward)
+  void* sw;              // (L,3N) T output s.w
+  LoadScalars* scal;
+  double* partials;
+  int skip_inactive;     // skip loads whose scal.active == 0 (recurrence use)
+  int use_mean;          // subtract scal.mean_r before scaling (projection P of the input)
+  int init;              // FZ finalizer: initialise rz instead of forming beta
+  int finalize_fz;       // FZ last block forms rz / beta (recurrence use only)
+};
+
+__device__ __forceinline__ bool load_on(const GreenArgs& A, int load) {
+  return A.skip_inactive ? (A.scal[load].active != 0) : true;
+}
+
+// ---------------------------------------------------------------------------- FX
+template <typename T>
+__global__ void __launch_bounds__(256) k_fx(const GreenArgs A) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int load = blockIdx.y;
+  if (!load_on(A, load)) return;
+  const int n = A.n, ns = A.ns, rb = A.geo.rb, pitch = n + 1;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int nl = 3 * rb / 2;  // complex lines
+  C* b0 = reinterpret_cast<C*>(smem_raw);
+  C* b1 = b0 + nl * pitch;
+  const size_t N = size_t(n) * n * n;
+  const size_t row0 = size_t(blockIdx.x) * rb;
+  const T* r = reinterpret_cast<const T*>(A.r) + size_t(load) * 3 * N;
+  const double* sc = A.scale;
+  double m[3] = {0.0, 0.0, 0.0};
+  if (A.use_mean) { m[0] = A.scal[load].mean_r[0]; m[1] = A.scal[load].mean_r[1]; m[2] = A.scal[load].mean_r[2]; }
+  const int total = rb * 3 * n;
+  const size_t gbase = row0 * n * 3;
+  for (int i = tid; i < total; i += nthr) {
+    const int rl = i / (3 * n);
+    const int rem = i - rl * 3 * n;
+    const int x = rem / 3, c = rem - 3 * (rem / 3);
+    const size_t g = gbase + i;
+    const T v = T(sc[g]) * (r[g] - T(m[c]));
+    const int rho = 3 * rl + c;
+    T* dst = reinterpret_cast<T*>(b0 + (rho >> 1) * pitch + x);
+    dst[rho & 1] = v;
+  }
+  __syncthreads();
+  const C* tw = reinterpret_cast<const C*>(A.tw);
+  C* res = fft_lines<T>(b0, b1, nl, pitch, A.plan, tw, false, tid, nthr);
+  // split: line rho=2l (real part) and rho=2l+1 (imaginary part)
+  C* spec = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * size_t(n) * n * ns;
+  const int tot2 = 3 * rb * ns;
+  for (int i = tid; i < tot2; i += nthr) {
+    const int rho = i / ns, k = i - rho * ns;
+    const int l = rho >> 1;
+    const C zk = res[l * pitch + k];
+    const C zn = res[l * pitch + (k == 0 ? 0 : n - k)];
+    C out;
+    if ((rho & 1) == 0) {  // (Z[k] + conj Z[n-k]) / 2
+      out.x = T(0.5) * (zk.x + zn.x); out.y = T(0.5) * (zk.y - zn.y);
+    } else {               // (Z[k] - conj Z[n-k]) / (2i)
+      out.x = T(0.5) * (zk.y + zn.y); out.y = T(0.5) * (zn.x - zk.x);
+    }
+    const int rl = rho / 3, c = rho - 3 * rl;
+    spec[(size_t(c) * n * n + row0 + rl) * ns + k] = out;
+  }
+}
+
+// ---------------------------------------------------------------------------- FY / IFY
+template <typename T, bool INV>
+__global__ void __launch_bounds__(256) k_fy(const GreenArgs A) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lc = blockIdx.z;  // load * 3 + component
+  const int load = lc / 3, c = lc - 3 * load;
+  if (!load_on(A, load)) return;
+  const int n = A.n, ns = A.ns, pitch = n + 1, kc = A.geo.kcy;
+  const int z = blockIdx.y;
+  const int k0 = blockIdx.x * kc;
+  const int kn = min(kc, ns - k0);
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  C* b0 = reinterpret_cast<C*>(smem_raw);
+  C* b1 = b0 + kc * pitch;
+  C* plane = reinterpret_cast<C*>(A.spec) + (size_t(load) * 3 + c) * size_t(n) * n * ns + size_t(z) * n * ns;
+  const int total = n * kn;
+  for (int i = tid; i < total; i += nthr) {
+    const int y = i / kn, kl = i - y * kn;
+    b0[kl * pitch + y] = plane[size_t(y) * ns + k0 + kl];
+  }
+  __syncthreads();
+  const C* tw = reinterpret_cast<const C*>(A.tw);
+  C* res = fft_lines<T>(b0, b1, kn, pitch, A.plan, tw, INV, tid, nthr);
+  for (int i = tid; i < total; i += nthr) {
+    const int y = i / kn, kl = i - y * kn;
+    plane[size_t(y) * ns + k0 + kl] = res[kl * pitch + y];
+  }
+}
+
+// ---------------------------------------------------------------------------- FZ (+ symbol)
+template <typename T>
+__global__ void __launch_bounds__(256) k_fz(const GreenArgs A) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int load = blockIdx.z;
+  if (!load_on(A, load)) return;
+  const int n = A.n, ns = A.ns, pitch = n + 1, kc = A.geo.kcz;
+  const int ky = blockIdx.y;
+  const int k0 = blockIdx.x * kc;
+  const int kn = min(kc, ns - k0);
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int nl = 3 * kn;
+  C* b0 = reinterpret_cast<C*>(smem_raw);
+  C* b1 = b0 + 3 * kc * pitch;
+  double* red = reinterpret_cast<double*>(b1 + 3 * kc * pitch);
+  const size_t plane = size_t(n) * n * ns;  // one component
+  C* sp = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * plane;
+  const int total = 3 * n * kn;
+  for (int i = tid; i < total; i += nthr) {
+    const int kl = i % kn, t = i / kn, z = t % n, c = t / n;
+    b0[(c * kn + kl) * pitch + z] = sp[c * plane + (size_t(z) * n + ky) * ns + k0 + kl];
+  }
+  __syncthreads();
+  const C* tw = reinterpret_cast<const C*>(A.tw);
+  C* res = fft_lines<T>(b0, b1, nl, pitch, A.plan, tw, false, tid, nthr);
+  // symbol multiply and Parseval partial sum
+  const T* sym = reinterpret_cast<const T*>(A.sym);
+  const size_t Nh = size_t(n) * n * ns;
+  double acc[1] = {0.0};
+  const int tot2 = n * kn;
+  for (int i = tid; i < tot2; i += nthr) {
+    const int kl = i % kn, kz = i / kn;
+    const int kx = k0 + kl;
+    const size_t kk = (size_t(kz) * n + ky) * ns + kx;
+    const T c0 = sym[kk], c1 = sym[Nh + kk], c2 = sym[2 * Nh + kk];
+    const T c3 = sym[3 * Nh + kk], c4 = sym[4 * Nh + kk], c5 = sym[5 * Nh + kk];
+    C* px = res + (0 * kn + kl) * pitch + kz;
+    C* py = res + (1 * kn + kl) * pitch + kz;
+    C* pz = res + (2 * kn + kl) * pitch + kz;
+    const C x = *px, y = *py, z = *pz;
+    C wx, wy, wz;
+    wx.x = c0 * x.x + c3 * y.x + c4 * z.x; wx.y = c0 * x.y + c3 * y.y + c4 * z.y;
+    wy.x = c3 * x.x + c1 * y.x + c5 * z.x; wy.y = c3 * x.y + c1 * y.y + c5 * z.y;
+    wz.x = c4 * x.x + c5 * y.x + c2 * z.x; wz.y = c4 * x.y + c5 * y.y + c2 * z.y;
+    const double wgt = (kx == 0 || kx == n / 2) ? 1.0 : 2.0;
+    acc[0] += wgt * (double(x.x) * wx.x + double(x.y) * wx.y + double(y.x) * wy.x + double(y.y) * wy.y +
+                     double(z.x) * wz.x + double(z.y) * wz.y);
+    *px = wx; *py = wy; *pz = wz;
+  }
+  __syncthreads();
+  C* other = (res == b0) ? b1 : b0;
+  C* res2 = fft_lines<T>(res, other, nl, pitch, A.plan, tw, true, tid, nthr);
+  for (int i = tid; i < total; i += nthr) {
+    const int kl = i % kn, t = i / kn, z = t % n, c = t / n;
+    sp[c * plane + (size_t(z) * n + ky) * ns + k0 + kl] = res2[(c * kn + kl) * pitch + z];
+  }
+  if (!A.finalize_fz) return;
+  block_sum<1>(acc, red);
+  const int nblk = gridDim.x * gridDim.y, blk = blockIdx.x + gridDim.x * blockIdx.y;
+  double* part = A.partials + size_t(load) * kPartialQ * kMaxPartials;
+  if (tid == 0) part[blk] = acc[0];
+  LoadScalars& S = A.scal[load];
+  if (!last_block(&S.ticket[kTicketFZ], nblk)) return;
+  if (tid < 32) {
+    const double rzn = warp_sum_partials(part, nblk);
+    if (tid == 0) {
+      if (A.init) {
+        S.beta = 0.0;
+      } else {
+        const double rz = S.rz;
+        S.beta = rzn / (rz != 0.0 ? rz : 1.0);
+      }
+      S.rz = rzn;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------- IFX
+template <typename T>
+__global__ void __launch_bounds__(256) k_ifx(const GreenArgs A) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int load = blockIdx.y;
+  if (!load_on(A, load)) return;
+  const int n = A.n, ns = A.ns, rb = A.geo.rb, pitch = n + 1;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int nl = 3 * rb / 2;
+  C* b0 = reinterpret_cast<C*>(smem_raw);
+  C* b1 = b0 + nl * pitch;
+  double* red = reinterpret_cast<double*>(b1 + nl * pitch);
+  const size_t N = size_t(n) * n * n;
+  const size_t row0 = size_t(blockIdx.x) * rb;
+  const C* spec = reinterpret_cast<const C*>(A.spec) + size_t(load) * 3 * size_t(n) * n * ns;
+  // Z[k] = A[k] + i B[k] over the full line, A/B Hermitian-extended; DC/Nyquist imaginary parts dropped
+  const int total = nl * n;
+  for (int i = tid; i < total; i += nthr) {
+    const int l = i / n, k = i - l * n;
+    C v[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int rho = 2 * l + h;
+      const int rl = rho / 3, c = rho - 3 * rl;
+      const C* src = spec + (size_t(c) * n * n + row0 + rl) * ns;
+      C val;
+      if (k < ns) {
+        val = src[k];
+        if (k == 0 || k == n / 2) val.y = T(0);
+      } else {
+        val = cconj(src[n - k]);
+      }
+      v[h] = val;
+    }
+    C z;
+    z.x = v[0].x - v[1].y;
+    z.y = v[0].y + v[1].x;
+    b0[l * pitch + k] = z;
+  }
+  __syncthreads();
+  const C* tw = reinterpret_cast<const C*>(A.tw);
+  C* res = fft_lines<T>(b0, b1, nl, pitch, A.plan, tw, true, tid, nthr);
+  T* sw = reinterpret_cast<T*>(A.sw) + size_t(load) * 3 * N;
+  const double* sc = A.scale;
+  double acc[3] = {0.0, 0.0, 0.0};
+  const int tot2 = rb * 3 * n;
+  const size_t gbase = row0 * n * 3;
+  for (int i = tid; i < tot2; i += nthr) {
+    const int rl = i / (3 * n);
+    const int rem = i - rl * 3 * n;
+    const int x = rem / 3, c = rem - 3 * (rem / 3);
+    const int rho = 3 * rl + c;
+    const C zz = res[(rho >> 1) * pitch + x];
+    const T w = (rho & 1) ? zz.y : zz.x;
+    const T o = T(sc[gbase + i]) * w;
+    sw[gbase + i] = o;
+    acc[c] += double(o);
+  }
+  block_sum<3>(acc, red);
+  const int nblk = gridDim.x;
+  double* part = A.partials + size_t(load) * kPartialQ * kMaxPartials + kMaxPartials;
+  if (tid == 0)
+    for (int k = 0; k < 3; ++k) part[k * kMaxPartials + blockIdx.x] = acc[k];
+  LoadScalars& S = A.scal[load];
+  if (!last_block(&S.ticket[kTicketIFX], nblk)) return;
+  if (tid < 32) {
+    double v[3];
+    for (int k = 0; k < 3; ++k) v[k] = warp_sum_partials(part + k * kMaxPartials, nblk);
+    if (tid == 0)
+      for (int k = 0; k < 3; ++k) S.mean_z[k] = v[k] / double(N);
+  }
+}
+
+// ---------------------------------------------------------------------------- host side
+static size_t smem_x(const pgj_ctx* c, size_t cb) {
+  const int nl = 3 * c->fg.rb / 2;
+  return 2 * size_t(nl) * (c->n + 1) * cb + 32 * 3 * 8 + 64;
+}
+static size_t smem_y(const pgj_ctx* c, size_t cb) { return 2 * size_t(c->fg.kcy) * (c->n + 1) * cb; }
+static size_t smem_z(const pgj_ctx* c, size_t cb) { return 2 * 3 * size_t(c->fg.kcz) * (c->n + 1) * cb + 32 * 8 + 64; }
+
+template <typename T>
+static int set_smem_limits() {
+  const int lim = 227 * 1024;
+  cudaFuncSetAttribute(k_fx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fy<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fy<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fz<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_ifx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  return check_launch();
+}
+
+int prepare_fft_kernels() {
+  int st = set_smem_limits<double>();
+  return st ? st : set_smem_limits<float>();
+}
+
+template <typename T>
+static int run_green(pgj_ctx* c, int loads, GreenArgs& A, cudaStream_t s) {
+  int st;
+  const size_t cb = 2 * sizeof(T);
+  const int n = c->n, ns = c->ns;
+  const FFTGeom& g = c->fg;
+  k_fx<T><<<dim3((n * n) / g.rb, loads), 256, smem_x(c, cb), s>>>(A);
+  if ((st = check_launch())) return st;
+  k_fy<T, false><<<dim3(g.nky, n, 3 * loads), 256, smem_y(c, cb), s>>>(A);
+  if ((st = check_launch())) return st;
+  k_fz<T><<<dim3(g.nkz, n, loads), 256, smem_z(c, cb), s>>>(A);
+  if ((st = check_launch())) return st;
+  k_fy<T, true><<<dim3(g.nky, n, 3 * loads), 256, smem_y(c, cb), s>>>(A);
+  if ((st = check_launch())) return st;
+  k_ifx<T><<<dim3((n * n) / g.rb, loads), 256, smem_x(c, cb), s>>>(A);
+  (void)ns;
+  return check_launch();
+}
+
+static GreenArgs green_args(pgj_ctx* c, int prec, const void* r) {
+  GreenArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.n = c->n; A.ns = c->ns; A.plan = c->plan; A.geo = c->fg;
+  A.r = r; A.scale = c->scale; A.spec = c->spec;
+  A.sym = prec == PGJ_FP32 ? static_cast<const void*>(c->symbol32) : static_cast<const void*>(c->symbol);
+  A.tw = prec == PGJ_FP32 ? static_cast<const void*>(static_cast<double2*>(c->tw) + c->n) : c->tw;
+  A.sw = c->sw; A.scal = c->scal; A.partials = c->partials;
+  return A;
+}
+
+int launch_green(pgj_ctx* c, int loads, int prec, const void* r, bool init, cudaStream_t s) {
+  GreenArgs A = green_args(c, prec, r);
+  A.skip_inactive = 1;
+  A.use_mean = 1;
+  A.init = init ? 1 : 0;
+  A.finalize_fz = 1;
+  return prec == PGJ_FP32 ? run_green<float>(c, loads, A, s) : run_green<double>(c, loads, A, s);
+}
+
+// z = P(s . w) = s.w - mean(s.w), from the sw buffer and the IFX finalizer's means.
+__global__ void k_project_out(int n, const double* __restrict__ sw, double* __restrict__ z, const LoadScalars* scal) {
+  const size_t N3 = 3 * size_t(n) * n * n;
+  const int load = blockIdx.y;
+  const double m0 = scal[load].mean_z[0], m1 = scal[load].mean_z[1], m2 = scal[load].mean_z[2];
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x) {
+    const int cc = int(i % 3);
+    z[size_t(load) * N3 + i] = sw[size_t(load) * N3 + i] - (cc == 0 ? m0 : (cc == 1 ? m1 : m2));
+  }
+}
+
+int launch_green_standalone(pgj_ctx* c, int loads, const double* r, double* z, cudaStream_t s) {
+  int st = launch_mean3(c, loads, r, 1, s);  // scal.mean_r
+  if (st) return st;
+  GreenArgs A = green_args(c, PGJ_FP64, r);
+  A.skip_inactive = 0;
+  A.use_mean = 1;
+  A.finalize_fz = 0;
+  if ((st = run_green<double>(c, loads, A, s))) return st;
+  k_project_out<<<dim3(296, loads), 256, 0, s>>>(c->n, static_cast<const double*>(c->sw), z, c->scal);
+  return check_launch();
+}
+
+// ---------------------------------------------------------------------------- tables
+int init_fft_tables(pgj_ctx* c, cudaStream_t s) {
+  const int n = c->n;
+  std::vector<double2> t64(n);
+  std::vector<float2> t32(n);
+  for (int k = 0; k < n; ++k) {
+    const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)k / (long double)n;
+    const double cr = (double)cosl(ang), ci = (double)sinl(ang);
+    t64[k] = make_double2(cr, ci);
+    t32[k] = make_float2((float)cr, (float)ci);
+  }
+  cudaError_t e = cudaMemcpyAsync(c->tw, t64.data(), n * sizeof(double2), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(static_cast<double2*>(c->tw) + n, t32.data(), n * sizeof(float2), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  return e == cudaSuccess ? PGJ_OK : set_cuda_error(e);
+}
+
+// FI HEX8 Green symbol: fi_coeff_kernel (formula_kernels.cu:104-126) with the half-angle tables
+// of formula_adapter.py:48-53, expanded densely with 1/N folded in (precision_kernels.cu:57-89).
+__global__ void k_symbol(int n, double lam, double mu, double* __restrict__ out, float* __restrict__ out32) {
+  const int ns = n / 2 + 1;
+  const size_t Nh = size_t(n) * n * ns;
+  const size_t k = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (k >= Nh) return;
+  const int kx = int(k % ns), ky = int((k / ns) % n), kz = int(k / (size_t(ns) * n));
+  const double h = 1.0 / n, pi = 3.14159265358979323846;
+  const int kk[3] = {kx, ky, kz};
+  double m[3], v[3], d[3];
+  double t = h * h * h, trace = 0.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    double sn, cs;
+    sincos(pi * kk[i] / n, &sn, &cs);
+    m[i] = cs * cs + sn * sn / 3;
+    t *= m[i];
+    v[i] = 2 * sn * cs / (h * m[i]);
+    d[i] = 4 * (sn * sn) * (sn * sn) / (3 * h * h * m[i] * m[i]);
+  }
+#pragma unroll
+  for (int i = 0; i < 3; ++i) trace += d[i] + v[i] * v[i];
+  trace *= t;
+  const double b = (lam + mu) * t;
+  double inv[3], den = 1.0;
+#pragma unroll
+  for (int i = 0; i < 3; ++i) {
+    inv[i] = k == 0 ? 0.0 : 1.0 / (mu * trace + (lam + mu) * t * d[i]);
+    den += b * v[i] * v[i] * inv[i];
+  }
+  const double beta = k == 0 ? 0.0 : b / den;
+  const double invN = 1.0 / (double(n) * n * n);
+  double w[3];
+#pragma unroll
+  for (int i = 0; i < 3; ++i) w[i] = inv[i] * v[i];
+  double cf[6];
+  cf[0] = (inv[0] - beta * w[0] * w[0]) * invN;
+  cf[1] = (inv[1] - beta * w[1] * w[1]) * invN;
+  cf[2] = (inv[2] - beta * w[2] * w[2]) * invN;
+  cf[3] = -beta * w[0] * w[1] * invN;
+  cf[4] = -beta * w[0] * w[2] * invN;
+  cf[5] = -beta * w[1] * w[2] * invN;
+#pragma unroll
+  for (int j = 0; j < 6; ++j) {
+    if (out) out[j * Nh + k] = cf[j];
+    if (out32) out32[j * Nh + k] = float(cf[j]);
+  }
+}
+
+int build_symbol(int n, double lam, double mu, double* sym, float* sym32, cudaStream_t s) {
+  const size_t Nh = size_t(n) * n * (n / 2 + 1);
+  k_symbol<<<unsigned((Nh + 255) / 256), 256, 0, s>>>(n, lam, mu, sym, sym32);
+  return check_launch();
+}
+
+}  // namespace pgj

@@ -1,0 +1,141 @@
+// Internal host-side interfaces shared by the libpgj translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <cstddef>
+#include <cstdint>
+#include "pgj_common.cuh"
+
+namespace pgj {
+
+struct FFTPlan {
+  int n;
+  int nst;
+  int radix[kMaxStages];
+};
+bool make_fft_plan(int n, FFTPlan* plan);
+
+// Launch geometry of the streaming stencil for a grid edge n.
+struct StencilGeom {
+  int ty;      // output node rows per block (block is n x (ty+1) threads)
+  int ntiles;  // tiles along y
+  int zc;      // output node planes per block
+  int nchunks; // chunks along z
+  int threads() const { return 0; }
+};
+StencilGeom stencil_geom(int n, int loads);
+
+// Geometry of the FFT passes.
+struct FFTGeom {
+  int rb;        // rows (z,y) per x-pass block
+  int kcy;       // kx columns per y-pass block
+  int nky;       // y-pass chunks
+  int kcz;       // kx columns per z-pass block
+  int nkz;       // z-pass chunks
+};
+FFTGeom fft_geom(int n, int elem_bytes);
+
+enum StencilMode { kPlain = 0, kPCG = 1, kResidual = 2 };
+
+struct StencilArgs {
+  int n, ty, zc;
+  const double* a;
+  const void* in;
+  void* out;
+  const double* f;             // residual mode: right-hand side
+  const int32_t* active_ext;   // plain mode: optional external mask
+  LoadScalars* scal;           // pcg / residual modes
+  double* partials;            // [load][4][nblk]
+  OpConst kc;
+  int iteration_cap;
+};
+
+// Partial-sum slots per load per kernel (blocks per load upper bound).
+constexpr int kMaxPartials = 4096;
+constexpr int kPartialQ = 4;
+// aux block: [0,24) stiffness diagonal per local node, [32,68) unit Voigt macros,
+// [128, 128 + kMaxPartials) scalar-reduction partials of the scale build.
+constexpr int kAuxVoigt = 32;
+constexpr int kAuxPartials = 128;
+constexpr int kAuxDoubles = kAuxPartials + kMaxPartials;
+
+struct Layout {
+  size_t a, scale, symbol, symbol32, tw, solutions, f, x, r, p, q, sw, spec, partials, scal, macros,
+      cond, r64, aux, total;
+};
+
+struct Graphs;
+
+}  // namespace pgj
+
+struct pgj_ctx {
+  int n, L, prec;
+  double lam, mu;
+  long long N;
+  int ns;
+  long long Nh;
+  pgj::OpConst kc;
+  pgj::FFTPlan plan;
+  pgj::StencilGeom sg;
+  pgj::FFTGeom fg;
+  pgj::Layout lay;
+  char* base;
+  size_t bytes;
+  // workspace views
+  double* a;
+  double* scale;
+  double* symbol;
+  float* symbol32;
+  void* tw;            // n complex twiddles: double2[n] then float2[n]
+  double* solutions;   // (L, 3N) fp64 warm starts
+  double* f;           // (L, 3N) fp64 right-hand sides
+  double* x;           // (L, 3N) fp64 iterate (plain) / refined solution (mixed)
+  void* r;             // (L, 3N) T
+  void* p;             // (L, 3N) T
+  void* q;             // (L, 3N) T
+  void* sw;            // (L, 3N) T  s . w (unprojected preconditioned residual)
+  void* spec;          // (L, 3, n, n, ns) complex T
+  double* partials;    // (L, kPartialQ * kMaxPartials)
+  pgj::LoadScalars* scal;  // L records
+  double* macros;      // (L, 6) device copy
+  int* cond;           // device flags (any active)
+  double* r64;         // mixed: fp64 residual (L, 3N)
+  double* aux;         // (64 + kMaxPartials) doubles: small staged tables and scalar reductions
+  double alpha;
+  double inner_rtol;
+  int last_refinements;
+  pgj::Graphs* graphs;
+};
+
+namespace pgj {
+// operator (pgj_operator.cu)
+int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, void* out, const double* f,
+                   const int32_t* active_ext, cudaStream_t s);
+int launch_rhs(pgj_ctx* c, int loads, const double* macros_dev, double* f, cudaStream_t s);
+int launch_scale(pgj_ctx* c, double alpha, cudaStream_t s);
+int launch_project_u(pgj_ctx* c, int loads, double* u, cudaStream_t s);
+// per-load component means of a DOF vector into scal.mean_u (which=0) or scal.mean_r (which=1)
+int launch_mean3(pgj_ctx* c, int loads, const double* v, int which, cudaStream_t s);
+int launch_norms(pgj_ctx* c, int loads, const double* f, double rtol, cudaStream_t s);
+// fft / green (pgj_fft.cu)
+int init_fft_tables(pgj_ctx* c, cudaStream_t s);
+int build_symbol(int n, double lam, double mu, double* sym, float* sym32, cudaStream_t s);
+int launch_green(pgj_ctx* c, int loads, int prec, const void* r, bool init, cudaStream_t s);
+int launch_green_standalone(pgj_ctx* c, int loads, const double* r, double* z, cudaStream_t s);
+// pcg (pgj_pcg.cu)
+int launch_update_ur(pgj_ctx* c, int loads, int prec, double* u64, void* uT, cudaStream_t s);
+int launch_update_p(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, cudaGraphConditionalHandle h,
+                    bool set_cond);
+int launch_init_mask(pgj_ctx* c, int loads, cudaStream_t s);
+// energy (pgj_energy.cu)
+int launch_energies(pgj_ctx* c, int loads, const double* u, const double* macros_dev, double* e, cudaStream_t s);
+int launch_effective_tensor(pgj_ctx* c, const double* u, double* C, double* e, cudaStream_t s);
+
+int set_cuda_error(cudaError_t e);
+// one-time kernel attributes (dynamic shared memory limits); called at context creation
+int prepare_stencil_kernels();
+int prepare_fft_kernels();
+inline int check_launch() {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? PGJ_OK : set_cuda_error(e);
+}
+}  // namespace pgj

@@ -1,0 +1,523 @@
+// Matrix-free periodic HEX8 operator, right-hand side, stiffness-diagonal scaling and projection.
+//
+// The operator q = K(a) p is a z-streaming stencil: a block owns full x-rows of n nodes and
+// `ty` output node rows (plus one halo element row), and marches a chunk of z-planes. Each
+// thread owns one element column. Per element plane it reads the four nodes of its upper face
+// from shared memory (the plane is staged with cp.async while the previous plane computes),
+// forms the 2D Hadamard face modes, combines them with the lower face modes kept in registers
+// (z-level), applies the modal element action, and splits the force modes into the parts that
+// belong to the lower and upper node planes. The lower plane is complete once the element
+// below it has been added; its y- and x-level transposes are exchanged through shared memory
+// in a fixed order, so the result is deterministic (no atomics, unlike the reference's
+// scatter in exp/asg_gpu_resident_20261103/scalar_fi.cu:14-36).
+#include "pgj_internal.h"
+#include <cmath>
+
+namespace pgj {
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+template <typename T> __device__ __forceinline__ void cp_async(T* dst, const T* src);
+template <> __device__ __forceinline__ void cp_async<double>(double* dst, const double* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src));
+}
+template <> __device__ __forceinline__ void cp_async<float>(float* dst, const float* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+__device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
+__device__ __forceinline__ void cp_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+StencilGeom stencil_geom(int n, int loads) {
+  StencilGeom g;
+  const int maxthreads = 512;
+  int best_ty = 1;
+  double best = 1e30;
+  for (int ty = 1; ty <= n && n * (ty + 1) <= maxthreads; ++ty) {
+    int tiles = (n + ty - 1) / ty;
+    double waste = double(tiles) * (ty + 1) / n;
+    if (waste < best - 1e-12) { best = waste; best_ty = ty; }
+  }
+  g.ty = best_ty;
+  g.ntiles = (n + g.ty - 1) / g.ty;
+  // aim for >= ~2 blocks per SM across the launch, z chunks of at least 4 planes
+  int want = (2 * 148 + loads * g.ntiles - 1) / (loads * g.ntiles);
+  int maxchunks = n / 4 > 0 ? n / 4 : 1;
+  int nch = want < 1 ? 1 : (want > maxchunks ? maxchunks : want);
+  g.zc = (n + nch - 1) / nch;
+  g.nchunks = (n + g.zc - 1) / g.zc;
+  return g;
+}
+
+template <typename T>
+__device__ __forceinline__ void stage_plane(T* buf, const T* in, int pz, int y0, int rows, int n, int tid, int nthr) {
+  const int rowlen = 3 * n;
+  const int total = rows * rowlen;
+  for (int i = tid; i < total; i += nthr) {
+    const int row = i / rowlen;
+    const int rem = i - row * rowlen;
+    int y = (y0 - 1 + row) % n;
+    if (y < 0) y += n;
+    cp_async(buf + i, in + (size_t(pz) * n + y) * size_t(rowlen) + rem);
+  }
+  cp_commit();
+}
+
+// Read the 4 nodes of the face (x..x+1, row..row+1) from a staged plane and form the face modes
+// F[f][c], f = mx + 2 my: F[0] = sum, F[1] = x-difference, F[2] = y-difference, F[3] = both.
+template <typename T>
+__device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, T (&F)[4][3], T (&own)[3]) {
+  const int xp = (x + 1 == n) ? 0 : x + 1;
+  const T* r0 = buf + row * 3 * n;
+  const T* r1 = r0 + 3 * n;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    const T u00 = r0[3 * x + c], u10 = r0[3 * xp + c], u01 = r1[3 * x + c], u11 = r1[3 * xp + c];
+    own[c] = u00;
+    const T sx0 = u10 + u00, dx0 = u10 - u00, sx1 = u11 + u01, dx1 = u11 - u01;
+    F[0][c] = sx1 + sx0;
+    F[1][c] = dx1 + dx0;
+    F[2][c] = sx1 - sx0;
+    F[3][c] = dx1 - dx0;
+  }
+}
+
+template <typename T, int MODE>
+__global__ void __launch_bounds__(512, 1) k_stencil(const StencilArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = A.n, TY = A.ty;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + n * ty, nthr = n * (TY + 1);
+  const int load = blockIdx.z;
+  const int nblk = gridDim.x * gridDim.y, blk = blockIdx.x + gridDim.x * blockIdx.y;
+  const size_t N = size_t(n) * n * n;
+  const int y0 = blockIdx.x * TY, z0 = blockIdx.y * A.zc;
+  const int zc = min(A.zc, n - z0);
+  const int ey = y0 - 1 + ty;
+  const int eyw = (ey + n) % n;
+  const bool out_row = (ty >= 1) && (ey < n);
+
+  bool act = true;
+  if (MODE == kPCG) act = A.scal[load].active != 0;
+  else if (A.active_ext) act = A.active_ext[load] != 0;
+  T* out = reinterpret_cast<T*>(A.out) + size_t(load) * 3 * N;
+  if (!act) {
+    if (MODE == kPlain && out_row) {
+      for (int z = z0; z < z0 + zc; ++z) {
+        T* o = out + 3 * ((size_t(z) * n + ey) * n + tx);
+        o[0] = T(0); o[1] = T(0); o[2] = T(0);
+      }
+    }
+    return;
+  }
+  const T* in = reinterpret_cast<const T*>(A.in) + size_t(load) * 3 * N;
+
+  const int planevals = (TY + 2) * 3 * n;
+  T* buf0 = reinterpret_cast<T*>(smem_raw);
+  T* buf1 = buf0 + planevals;
+  T* upy = buf1 + planevals;              // (TY+1) * n * 6
+  T* upx = upy + (TY + 1) * n * 6;         // (TY+1) * n * 3
+  double* red = reinterpret_cast<double*>(upx + (TY + 1) * n * 3 + 2);  // 32 * 4, 16-byte padded
+  red = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(red) + 15) & ~uintptr_t(15));
+
+  // prologue: planes z0-1 and z0
+  stage_plane(buf0, in, (z0 - 1 + n) % n, y0, TY + 2, n, tid, nthr);
+  stage_plane(buf1, in, z0 % n, y0, TY + 2, n, tid, nthr);
+  cp_wait_one();
+  __syncthreads();
+  T F0[4][3], own[3], dummy[3];
+  face_modes(buf0, ty, tx, n, F0, dummy);
+  T Up[4][3];
+#pragma unroll
+  for (int f = 0; f < 4; ++f)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) Up[f][c] = T(0);
+#pragma unroll
+  for (int c = 0; c < 3; ++c) own[c] = T(0);
+
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  const double* aa = A.a;
+
+  for (int s = 0; s <= zc; ++s) {
+    const int ez = z0 - 1 + s;           // element plane
+    const int ezw = (ez + n) % n;
+    const T ae = T(__ldg(aa + (size_t(ezw) * n + eyw) * n + tx));
+    cp_wait_all();
+    __syncthreads();
+    T* cur = ((s + 1) & 1) ? buf1 : buf0;
+    if (s < zc) stage_plane(((s & 1) ? buf1 : buf0), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
+
+    T F1[4][3], own1[3];
+    face_modes(cur, ty, tx, n, F1, own1);
+    // element modes: z level
+    T Q[8][3];
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        Q[f][c] = F1[f][c] + F0[f][c];
+        Q[f + 4][c] = F1[f][c] - F0[f][c];
+      }
+    T P[8][3];
+    element_modal<T>(Q, ae, A.kc, P);
+    // z-level transpose: U -> upper plane (ez+1), D -> lower plane (ez)
+    T U[4][3], G[4][3];
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        U[f][c] = P[f][c] + P[f + 4][c];
+        G[f][c] = (P[f][c] - P[f + 4][c]) + Up[f][c];
+      }
+    if (s >= 1) {
+      // output plane ez: y level
+      T R[2][3];
+#pragma unroll
+      for (int mx = 0; mx < 2; ++mx)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          upy[(ty * n + tx) * 6 + mx * 3 + c] = G[mx][c] + G[mx + 2][c];
+          R[mx][c] = G[mx][c] - G[mx + 2][c];
+        }
+      __syncthreads();
+      T qx[3];
+      if (ty >= 1) {
+#pragma unroll
+        for (int mx = 0; mx < 2; ++mx)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) R[mx][c] += upy[((ty - 1) * n + tx) * 6 + mx * 3 + c];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          upx[(ty * n + tx) * 3 + c] = R[0][c] + R[1][c];
+          qx[c] = R[0][c] - R[1][c];
+        }
+      }
+      __syncthreads();
+      if (out_row) {
+        const int xm = tx == 0 ? n - 1 : tx - 1;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) qx[c] += upx[(ty * n + xm) * 3 + c];
+        const size_t node = (size_t(ez) * n + ey) * n + tx;
+        T* o = out + 3 * node;
+        if (MODE == kResidual) {
+          const double* fl = A.f + size_t(load) * 3 * N + 3 * node;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const double rv = fl[c] - double(qx[c]);
+            o[c] = T(rv);
+            acc[0] += rv * rv;
+            acc[1 + c] += rv;
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) o[c] = qx[c];
+          if (MODE == kPCG) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[0] += double(own[c]) * double(qx[c]);
+          }
+        }
+      }
+    }
+#pragma unroll
+    for (int f = 0; f < 4; ++f)
+#pragma unroll
+      for (int c = 0; c < 3; ++c) { F0[f][c] = F1[f][c]; Up[f][c] = U[f][c]; }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) own[c] = own1[c];
+  }
+
+  if (MODE == kPlain) return;
+  block_sum<4>(acc, red);
+  double* part = A.partials + size_t(load) * kPartialQ * kMaxPartials;
+  if (tid == 0) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) part[k * kMaxPartials + blk] = acc[k];
+  }
+  LoadScalars& S = A.scal[load];
+  if (!last_block(&S.ticket[kTicketApply], nblk)) return;
+  if (tid < 32) {
+    if (MODE == kPCG) {
+      const double den = warp_sum_partials(part, nblk);
+      if (tid == 0) {
+        const double rz = S.rz;
+        const bool valid = isfinite(den) && den > 0.0 && isfinite(rz) && rz > 0.0;
+        S.failed = valid ? 0 : 1;
+        S.alpha = valid ? rz / den : 0.0;
+      }
+    } else {
+      double v[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) v[k] = warp_sum_partials(part + k * kMaxPartials, nblk);
+      if (tid == 0) {
+        S.res2 = v[0];
+        S.absolute = sqrt(v[0]);
+        const double inv = 1.0 / double(N);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) S.mean_r[c] = v[1 + c] * inv;
+      }
+    }
+  }
+}
+
+int prepare_stencil_kernels() {
+  const int lim = 227 * 1024;
+  cudaFuncSetAttribute(k_stencil<float, kPlain>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<float, kPCG>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<double, kPlain>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<double, kPCG>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<double, kResidual>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  return check_launch();
+}
+
+int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, void* out, const double* f,
+                   const int32_t* active_ext, cudaStream_t s) {
+  const int n = c->n;
+  StencilArgs A;
+  A.n = n; A.ty = c->sg.ty; A.zc = c->sg.zc;
+  A.a = c->a; A.in = in; A.out = out; A.f = f; A.active_ext = active_ext;
+  A.scal = c->scal; A.partials = c->partials; A.kc = c->kc; A.iteration_cap = 4000;
+  dim3 grid(c->sg.ntiles, c->sg.nchunks, loads), block(n, c->sg.ty + 1);
+  const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
+  const size_t smem = tsz * (size_t(2) * (c->sg.ty + 2) * 3 * n + size_t(c->sg.ty + 1) * n * 9) + 32 * 4 * 8 + 64;
+  if (c->sg.ntiles * c->sg.nchunks > kMaxPartials) return PGJ_ERR_UNSUPPORTED;
+  if (prec == PGJ_FP32) {
+    switch (mode) {
+      case kPlain: k_stencil<float, kPlain><<<grid, block, smem, s>>>(A); break;
+      case kPCG: k_stencil<float, kPCG><<<grid, block, smem, s>>>(A); break;
+      default: return PGJ_ERR_ARGUMENT;
+    }
+  } else {
+    switch (mode) {
+      case kPlain: k_stencil<double, kPlain><<<grid, block, smem, s>>>(A); break;
+      case kPCG: k_stencil<double, kPCG><<<grid, block, smem, s>>>(A); break;
+      case kResidual: k_stencil<double, kResidual><<<grid, block, smem, s>>>(A); break;
+      default: return PGJ_ERR_ARGUMENT;
+    }
+  }
+  return check_launch();
+}
+
+// --------------------------------------------------------------------------- right-hand side
+// f(node) = -V sum over the 8 elements e = node - b of B_c(b)^T (a_e C0 eps), B_c the element-centre
+// gradient (+-1/(4h) per axis); same arithmetic as hybrid_kernels.cu:50-68.
+__global__ void k_rhs(int n, int loads, const double* __restrict__ a, const double* __restrict__ macros,
+                      double lam, double mu, double* __restrict__ f) {
+  const size_t N = size_t(n) * n * n;
+  const size_t node = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int load = blockIdx.y;
+  if (node >= N || load >= loads) return;
+  const int x = int(node % n), y = int((node / n) % n), z = int(node / (size_t(n) * n));
+  const double* m = macros + 6 * load;
+  // C0 eps (Voigt, engineering shear)
+  const double tr = m[0] + m[1] + m[2];
+  double s0[6];
+  s0[0] = lam * tr + 2 * mu * m[0];
+  s0[1] = lam * tr + 2 * mu * m[1];
+  s0[2] = lam * tr + 2 * mu * m[2];
+  s0[3] = mu * m[3]; s0[4] = mu * m[4]; s0[5] = mu * m[5];
+  const double h = 1.0 / n, g = 1.0 / (4 * h), vol = h * h * h;
+  double fx = 0, fy = 0, fz = 0;
+#pragma unroll
+  for (int b = 0; b < 8; ++b) {
+    const int ex = wrapi(x - (b & 1), n), eyy = wrapi(y - ((b >> 1) & 1), n), ez = wrapi(z - ((b >> 2) & 1), n);
+    const double ae = a[(size_t(ez) * n + eyy) * n + ex];
+    const double dx = (b & 1) ? g : -g, dy = (b & 2) ? g : -g, dz = (b & 4) ? g : -g;
+    double s[6];
+#pragma unroll
+    for (int k = 0; k < 6; ++k) s[k] = ae * s0[k];
+    fx -= vol * (dx * s[0] + dy * s[5] + dz * s[4]);
+    fy -= vol * (dx * s[5] + dy * s[1] + dz * s[3]);
+    fz -= vol * (dx * s[4] + dy * s[3] + dz * s[2]);
+  }
+  double* o = f + size_t(load) * 3 * N + 3 * node;
+  o[0] = fx; o[1] = fy; o[2] = fz;
+}
+
+int launch_rhs(pgj_ctx* c, int loads, const double* macros_dev, double* f, cudaStream_t s) {
+  const size_t N = size_t(c->N);
+  dim3 grid(unsigned((N + 255) / 256), loads);
+  k_rhs<<<grid, 256, 0, s>>>(c->n, loads, c->a, macros_dev, c->lam, c->mu, f);
+  return check_launch();
+}
+
+// --------------------------------------------------------------------------- norms / targets
+// ||f|| per load, target^2 = max(rtol ||f||, 1e-13/sqrt(n))^2; resets iteration counters and
+// latches (resident.py:187-191).
+__global__ void k_norms(int n, const double* __restrict__ f, double rtol, LoadScalars* scal, double* partials) {
+  const size_t N3 = 3 * size_t(n) * n * n;
+  const int load = blockIdx.y;
+  const double* fl = f + size_t(load) * N3;
+  double acc[1] = {0.0};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x) {
+    const double v = fl[i];
+    acc[0] += v * v;
+  }
+  __shared__ double red[32];
+  block_sum<1>(acc, red);
+  double* part = partials + size_t(load) * kPartialQ * kMaxPartials;
+  if (threadIdx.x == 0) part[blockIdx.x] = acc[0];
+  LoadScalars& S = scal[load];
+  if (!last_block(&S.ticket[kTicketAux], gridDim.x)) return;
+  if (threadIdx.x < 32) {
+    const double s2 = warp_sum_partials(part, gridDim.x);
+    if (threadIdx.x == 0) {
+      const double norm = sqrt(s2);
+      const double t = fmax(norm * rtol, 1e-13 / sqrt(double(n)));
+      S.norm = norm;
+      S.target2 = t * t;
+      S.iterations = 0;
+      S.bad = 0;
+      S.failed = 0;
+      S.active = 0;
+    }
+  }
+}
+
+int launch_norms(pgj_ctx* c, int loads, const double* f, double rtol, cudaStream_t s) {
+  dim3 grid(148, loads);
+  k_norms<<<grid, 256, 0, s>>>(c->n, f, rtol, c->scal, c->partials);
+  return check_launch();
+}
+
+// --------------------------------------------------------------------------- projection of u
+// mean over nodes per component, then subtract (certification projection, resident.py:133-134).
+__global__ void k_mean3(int n, const double* __restrict__ u, int which, LoadScalars* scal, double* partials) {
+  const size_t N = size_t(n) * n * n;
+  const int load = blockIdx.y;
+  const double* ul = u + size_t(load) * 3 * N;
+  double acc[3] = {0.0, 0.0, 0.0};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+    acc[0] += ul[3 * i]; acc[1] += ul[3 * i + 1]; acc[2] += ul[3 * i + 2];
+  }
+  __shared__ double red[96];
+  block_sum<3>(acc, red);
+  double* part = partials + size_t(load) * kPartialQ * kMaxPartials;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 3; ++k) part[k * kMaxPartials + blockIdx.x] = acc[k];
+  LoadScalars& S = scal[load];
+  if (!last_block(&S.ticket[kTicketAux], gridDim.x)) return;
+  if (threadIdx.x < 32) {
+    double v[3];
+    for (int k = 0; k < 3; ++k) v[k] = warp_sum_partials(part + k * kMaxPartials, gridDim.x);
+    if (threadIdx.x == 0) {
+      double* dst = which ? S.mean_r : S.mean_u;
+      for (int k = 0; k < 3; ++k) dst[k] = v[k] / double(N);
+    }
+  }
+}
+
+__global__ void k_sub_mean3(int n, double* __restrict__ u, const LoadScalars* scal) {
+  const size_t N3 = 3 * size_t(n) * n * n;
+  const int load = blockIdx.y;
+  double* ul = u + size_t(load) * N3;
+  const double m0 = scal[load].mean_u[0], m1 = scal[load].mean_u[1], m2 = scal[load].mean_u[2];
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x) {
+    const int c = int(i % 3);
+    ul[i] -= (c == 0 ? m0 : (c == 1 ? m1 : m2));
+  }
+}
+
+int launch_mean3(pgj_ctx* c, int loads, const double* v, int which, cudaStream_t s) {
+  dim3 grid(148, loads);
+  k_mean3<<<grid, 256, 0, s>>>(c->n, v, which, c->scal, c->partials);
+  return check_launch();
+}
+
+int launch_project_u(pgj_ctx* c, int loads, double* u, cudaStream_t s) {
+  int st = launch_mean3(c, loads, u, 0, s);
+  if (st) return st;
+  dim3 grid2(296, loads);
+  k_sub_mean3<<<grid2, 256, 0, s>>>(c->n, u, c->scal);
+  return check_launch();
+}
+
+// --------------------------------------------------------------------------- diagonal scaling
+// log d(node, c), d = sum_b a(node - b) diag(Ke)[b][c]; partial sums of log d for the mean.
+__global__ void k_logdiag(int n, const double* __restrict__ a, const double* __restrict__ ed, double* __restrict__ out,
+                          LoadScalars* scal, double* partials) {
+  const size_t N = size_t(n) * n * n;
+  double acc[1] = {0.0};
+  for (size_t node = size_t(blockIdx.x) * blockDim.x + threadIdx.x; node < N; node += size_t(gridDim.x) * blockDim.x) {
+    const int x = int(node % n), y = int((node / n) % n), z = int(node / (size_t(n) * n));
+    double d[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      const int ex = wrapi(x - (b & 1), n), eyy = wrapi(y - ((b >> 1) & 1), n), ez = wrapi(z - ((b >> 2) & 1), n);
+      const double ae = a[(size_t(ez) * n + eyy) * n + ex];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) d[c] += ae * ed[3 * b + c];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const double q = log(d[c]);
+      out[3 * node + c] = q;
+      acc[0] += q;
+    }
+  }
+  __shared__ double red[32];
+  block_sum<1>(acc, red);
+  if (threadIdx.x == 0) partials[blockIdx.x] = acc[0];
+  if (!last_block(&scal[0].ticket[kTicketAux2], gridDim.x)) return;
+  if (threadIdx.x < 32) {
+    const double s2 = warp_sum_partials(partials, gridDim.x);
+    if (threadIdx.x == 0) partials[kMaxPartials - 1] = s2 / double(3 * N);
+  }
+}
+
+__global__ void k_exp_scale(size_t count, double* __restrict__ q, const double* __restrict__ mean, double coef) {
+  const double m = *mean;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += size_t(gridDim.x) * blockDim.x)
+    q[i] = exp(coef * (q[i] - m));
+}
+
+__global__ void k_fill(size_t count, double* __restrict__ q, double v) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < count; i += size_t(gridDim.x) * blockDim.x) q[i] = v;
+}
+
+// diag(Ke) per local node b (bit order), 2x2x2 Gauss, isotropic C0; host-side constant.
+void element_diagonal(int n, double lam, double mu, double* ed) {
+  const double g = 1.0 / std::sqrt(3.0);
+  for (int i = 0; i < 24; ++i) ed[i] = 0.0;
+  for (int q = 0; q < 8; ++q) {
+    const double p[3] = {0.5 + ((q & 1) ? 0.5 : -0.5) * g, 0.5 + ((q & 2) ? 0.5 : -0.5) * g,
+                         0.5 + ((q & 4) ? 0.5 : -0.5) * g};
+    for (int b = 0; b < 8; ++b) {
+      const int v[3] = {b & 1, (b >> 1) & 1, (b >> 2) & 1};
+      double fac[3], grad[3];
+      for (int d = 0; d < 3; ++d) fac[d] = v[d] ? p[d] : 1 - p[d];
+      for (int d = 0; d < 3; ++d) {
+        double prod = 1.0;
+        for (int e = 0; e < 3; ++e) if (e != d) prod *= fac[e];
+        grad[d] = (2 * v[d] - 1) * prod * n;
+      }
+      // diagonal of B^T C B for the x, y, z dofs of node b
+      const double l2m = lam + 2 * mu;
+      ed[3 * b + 0] += l2m * grad[0] * grad[0] + mu * (grad[1] * grad[1] + grad[2] * grad[2]);
+      ed[3 * b + 1] += l2m * grad[1] * grad[1] + mu * (grad[0] * grad[0] + grad[2] * grad[2]);
+      ed[3 * b + 2] += l2m * grad[2] * grad[2] + mu * (grad[0] * grad[0] + grad[1] * grad[1]);
+    }
+  }
+  const double vol8 = 1.0 / (double(n) * n * n) / 8.0;
+  for (int i = 0; i < 24; ++i) ed[i] *= vol8;
+}
+
+int launch_scale(pgj_ctx* c, double alpha, cudaStream_t s) {
+  const size_t count = 3 * size_t(c->N);
+  if (alpha == 0.0) {
+    k_fill<<<296, 256, 0, s>>>(count, c->scale, 1.0);
+    return check_launch();
+  }
+  double ed[24];
+  element_diagonal(c->n, c->lam, c->mu, ed);
+  double* edd = c->aux;  // 24 diagonal entries, staged in the context's aux block
+  cudaError_t e = cudaMemcpyAsync(edd, ed, sizeof(ed), cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  k_logdiag<<<296, 256, 0, s>>>(c->n, c->a, edd, c->scale, c->scal, c->aux + kAuxPartials);
+  int st = check_launch();
+  if (st) return st;
+  k_exp_scale<<<296, 256, 0, s>>>(count, c->scale, c->aux + kAuxPartials + kMaxPartials - 1, -0.5 * alpha);
+  return check_launch();
+}
+
+}  // namespace pgj
