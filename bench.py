@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Certified 6-load homogenizations/s (p50/p99 latency) on B200.
+
+Workload (one step): a seeded synthetic design at n=64 (N(0,1) noise, periodic Gaussian sigma=n/16,
+quantile threshold to vf=0.35, logistic width 0.1; SIMP p=3, E0=1, Emin=1e-6; paper medium
+E=1, nu=0.3), the six unit Voigt loads as parallel PCG recurrences from a zero start, partial
+Green-Jacobi alpha=0.5, every load certified to relative true residual <= 1e-8, then C_H (6x6).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl pgj|reference]
+
+* value        device-resident inputs (designs already in HBM), CUDA-event timed on the stream.
+* e2e          same metric through the public API (PaperResident) with the design copied from
+               pinned host memory and C_H copied back every step.
+* roofline     dominant kernel of the PCG iteration, timed live with CUDA events (pgj_profile_iteration).
+* cpu_baseline the CPU restatement of the reference arithmetic (oracle/pgj_oracle.py) on a
+               bounded sample, extrapolated to one homogenization.
+Multi-GPU: replicas only (independent designs per rank, no collective on the data path); the
+timing is max-over-ranks; value = all homogenizations / that time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+METRIC = "certified 6-load homogenizations/s & p50/p99 latency, mixed vs FP64 at 1e-8"
+UNIT = "homogenizations/s"
+N_GRID, EMIN, ALPHA, RTOL, NSEEDS = 64, 1e-6, 0.5, 1e-8, 5
+FALLBACK_HBM = 6650.0
+L2_BYTES = 126e6
+
+
+def workload_config(extra=None):
+    cfg = {"workload": f"periodic HEX8 homogenization n={N_GRID}, 6 Voigt loads parallel, FP64 PCG, "
+                       f"alpha={ALPHA}, Emin={EMIN:g}, zero start, rtol={RTOL:g}, C_H",
+           "n": N_GRID, "loads": 6, "emin": EMIN, "alpha": ALPHA, "rtol": RTOL, "vf": 0.35,
+           "designs": f"seeds rank*1000+0..{NSEEDS - 1}, cycled", "medium": "E=1, nu=0.3",
+           "l2": "working set per homogenization ~310 MB > 126 MB L2 (no flush needed)",
+           "parallelism": "replicas"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+def peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[3:7]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def traffic_from_profiles(kernel):
+    p = ROOT / "profiles" / "traffic_n64.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return d.get(kernel)
+    return None
+
+
+# ------------------------------------------------------------------------------------------ CPU
+def cpu_sample(n=N_GRID, seed=0, iters=4, its_full=None):
+    """Oracle timing sample: setup + `iters` PCG iterations + one energy evaluation, extrapolated."""
+    sys.path.insert(0, str(ROOT / "oracle"))
+    import pgj_oracle as O
+
+    from __graft_entry__ import load_package
+
+    a = load_package().baseline_design(n, seed, EMIN)
+    lam, mu = O.PAPER
+    t0 = time.perf_counter()
+    prob = O.Problem(a, lam, mu, ALPHA)
+    f = O.rhs(prob.a, np.eye(6), lam, mu)
+    t1 = time.perf_counter()
+    u, infos, _ = O.solve_batch(prob, f, max_iterations=0)  # certification + init only
+    t2 = time.perf_counter()
+    O.solve_batch(prob, f, max_iterations=iters)
+    t3 = time.perf_counter()
+    aff = O.affine(n, np.eye(6))
+    O.energies(u[:1], aff[:1], n, lam, mu)
+    t4 = time.perf_counter()
+    per_iter = max((t3 - t2) - (t2 - t1), 1e-9) / iters
+    setup = (t1 - t0) + (t2 - t1)  # problem setup, rhs, certification + initialisation + final certification
+    its = its_full if its_full is not None else 300
+    total = setup + its * per_iter + 21 * (t4 - t3)  # C_H by polarisation: 21 single-load energy evaluations
+    return dict(value=1.0 / total, seconds_per_homogenization=total, per_iteration_s=per_iter, setup_s=setup,
+                energy_s=(t4 - t3), iterations=its)
+
+
+# ------------------------------------------------------------------------------------------ GPU
+def designs_for(rank, pkg):
+    return [pkg.baseline_design(N_GRID, rank * 1000 + k, EMIN) for k in range(NSEEDS)]
+
+
+def run_gpu(args, rank, world, local_rank):
+    import torch
+
+    from __graft_entry__ import load_package
+
+    pkg = load_package()
+    torch.cuda.set_device(local_rank)
+    stream = torch.cuda.Stream()
+    host = designs_for(rank, pkg)
+    lam, mu = pkg.PAPER_MEDIUM
+    eye6 = np.eye(6)
+    with torch.cuda.stream(stream):
+        dev = [torch.tensor(a, device="cuda") for a in host]
+        op = pkg.Operator(N_GRID, 6, lam, mu)
+        u = torch.zeros((6, 3 * N_GRID ** 3), dtype=torch.float64, device="cuda")
+        C = torch.empty((6, 6), dtype=torch.float64, device="cuda")
+        iters, launches = [], []
+
+        def step(k, record=True):
+            op.set_material(dev[k % NSEEDS])
+            op.set_alpha(ALPHA)
+            u.zero_()
+            infos, st = op.solve(eye6, RTOL, u)
+            if st != 0:
+                raise RuntimeError(("certification failed", infos))
+            C.copy_(op.effective_tensor(u))
+            if record:
+                iters.append([i["iterations"] for i in infos])
+                launches.append(op.last_launches() + 3)  # + scale build (2) + C_H (1)
+
+        for k in range(args.warmup):
+            step(k, record=False)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+        with ClockSampler(local_rank) as clocks:
+            ev[0].record(stream)
+            for k in range(args.steps):
+                step(k)
+                ev[k + 1].record(stream)
+            torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        lat = [ev[k].elapsed_time(ev[k + 1]) for k in range(args.steps)]
+        total_ms = ev[0].elapsed_time(ev[-1])
+
+        # end to end through the public API: pinned host design in, C_H out, every step
+        r = pkg.PaperResident(None, N_GRID, "shear", 0.35, emin=EMIN, load_mode="parallel")
+        pinned = [torch.from_numpy(a).pin_memory() for a in host]
+        c_host = torch.empty((6, 6), dtype=torch.float64).pin_memory()
+
+        def e2e_step(k):
+            d = pinned[k % NSEEDS].to("cuda", non_blocking=True)
+            r.material(d)
+            r.select(str(ALPHA))
+            r.solutions.zero_()
+            r.solve(RTOL)
+            c_host.copy_(r.effective_tensor(), non_blocking=True)
+            torch.cuda.current_stream().synchronize()
+
+        for k in range(args.warmup):
+            e2e_step(k)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for k in range(args.steps):
+            e2e_step(k)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+        prof = op.profile_iteration(eye6, reps=20) if rank == 0 else None
+        torch.cuda.synchronize()
+
+    if world > 1:
+        t = torch.tensor([total_ms, e2e_ms], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms, e2e_ms = float(t[0]), float(t[1])
+    return dict(total_ms=total_ms, e2e_ms=e2e_ms, lat=lat, iters=iters, launches=launches, prof=prof,
+                clocks=clocks.summary(), h2d=host[0].nbytes, d2h=36 * 8)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["pgj", "reference"], default="pgj")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", 0))
+    world = int(os.environ.get("WORLD_SIZE", 1))
+    local_rank = int(os.environ.get("LOCAL_RANK", 0))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        samples = []
+        t_start = time.perf_counter()
+        for k in range(args.warmup + args.steps):
+            s = cpu_sample(seed=k % NSEEDS, iters=2)
+            if k >= args.warmup:
+                samples.append(s)
+        vals = [s["value"] for s in samples]
+        value = float(np.mean(vals))
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": 1000.0 / value, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": workload_config({"extrapolation": "per-step sample: setup + 2 PCG iterations + 1 energy "
+                                                            "evaluation, scaled to 300 iterations and 21 energies"}),
+                "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                 "sample": "CPU restatement of the reference arithmetic (NumPy/SciPy, all host "
+                                           "threads); per step a bounded sample extrapolated to one homogenization"},
+                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                "wall_s": time.perf_counter() - t_start}
+        print(json.dumps(line), flush=True)
+        return
+
+    import torch
+
+    if world > 1:
+        import datetime
+
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    res = run_gpu(args, rank, world, local_rank)
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    homs = args.steps * world
+    value = homs / (res["total_ms"] / 1000.0)
+    e2e = homs / (res["e2e_ms"] / 1000.0)
+    lat = sorted(res["lat"])
+    p50 = float(np.percentile(lat, 50))
+    p99 = float(np.percentile(lat, 99))
+    hbm, kind = peaks()
+    prof = res["prof"]
+    dom = max(prof, key=lambda k: prof[k]["ms"])
+    achieved = prof[dom]["bytes"] / (prof[dom]["ms"] * 1e-3) / 1e9
+    iter_ms = sum(v["ms"] for v in prof.values())
+    its = np.array(res["iters"])
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": res["total_ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(), "p50_ms": p50, "p99_ms": p99,
+            "iterations_per_load_mean": float(its.mean()), "iterations_max_mean": float(its.max(1).mean()),
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"]},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                         "frac": achieved / hbm, "peak_kind": kind, "traffic": traffic_from_profiles(dom),
+                         "iteration_ms": iter_ms,
+                         "kernels": {k: {"ms": v["ms"], "GBps": v["bytes"] / (v["ms"] * 1e-3) / 1e9}
+                                     for k, v in prof.items()}},
+            "gpu_launches": int(sum(res["launches"])), "clocks": res["clocks"]}
+    if world == 1 and not args.no_cpu:
+        cb = cpu_sample(its_full=int(its.max(1).mean()))
+        line["cpu_baseline"] = {"value": cb["value"], "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"oracle n=64 6 loads: setup + 4 PCG iterations + 1 energy evaluation, "
+                                          f"extrapolated to {cb['iterations']} iterations (the GPU's mean max count) "
+                                          f"and 21 energies; {cb['per_iteration_s']:.3f} s/iteration"}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

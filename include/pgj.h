@@ -120,6 +120,18 @@ int pgj_set_inner_rtol(pgj_ctx* ctx, double inner_rtol);
 /* Number of refinement sweeps taken by the last pgj_solve (1 for PGJ_FP64). */
 int pgj_last_refinements(pgj_ctx* ctx);
 
+/* Kernel launches issued by the last pgj_solve (graph nodes included), for launch accounting. */
+long long pgj_last_launches(pgj_ctx* ctx);
+/* Measurement hook (no reference counterpart; the reference times stages with CUDA events,
+ * exp/asg_gpu_resident_20261103/run.py:29-53): starts a zero-start solve of `loads` macros and
+ * times each kernel of the PCG iteration separately with CUDA events on `stream`, over `reps`
+ * iterations. Writes PGJ_PROFILE_KERNELS mean durations (ms) and algorithmic bytes per launch
+ * (HOST arrays) in the order: operator, update_ur, fft_x, fft_y, fft_z+symbol, ifft_y, ifft_x,
+ * update_p. Leaves the context's iterate undefined (the next pgj_solve starts from its u). */
+#define PGJ_PROFILE_KERNELS 8
+int pgj_profile_iteration(pgj_ctx* ctx, int loads, const double* macros, int reps, double* ms, double* bytes,
+                          void* stream);
+
 /* ------------------------------------------------------------------ responses
  * Per-element energies e_l = v^T Ke(C0) v / h^3, v = u_l + A_l (affine macro field), for each of
  * `loads` (u, macros); e: (loads, N) device (energy.cu evaluate,

@@ -61,6 +61,8 @@ SIGNATURES = {
     "pgj_solve": (C.c_int, [vp, C.c_int, vp, f64, vp, C.POINTER(LoadInfo), vp]),
     "pgj_set_inner_rtol": (C.c_int, [vp, f64]),
     "pgj_last_refinements": (C.c_int, [vp]),
+    "pgj_last_launches": (C.c_longlong, [vp]),
+    "pgj_profile_iteration": (C.c_int, [vp, C.c_int, vp, C.c_int, vp, vp, vp]),
     "pgj_energies": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
     "pgj_effective_tensor": (C.c_int, [vp, vp, vp, vp]),
     "pgj_cone_filter": (C.c_int, [C.c_int, vp, vp, C.c_int, vp, vp, vp]),

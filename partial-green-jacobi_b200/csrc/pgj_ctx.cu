@@ -340,11 +340,17 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
   std::vector<LoadScalars> h(loads);
   std::vector<int> ok(loads, 0);
   int restarts = 0;
+  int body[2] = {0, 0};
+  long long launches = 2 + 3;  // rhs + norms, initial certification
   for (;;) {
     if ((e = cudaGraphLaunch(c->graphs->attempt, s)) != cudaSuccess) return set_cuda_error(e);
     e = cudaMemcpyAsync(h.data(), c->scal, sizeof(LoadScalars) * loads, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(body, c->cond, sizeof(body), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return set_cuda_error(e);
+    // attempt: init mask + 5 Green passes + p init, 8 kernels per loop body, 3 certification kernels
+    launches += 7 + 8LL * body[0] + 3;
+    if (body[1]) return PGJ_ERR_ITERATION_CAP;
     bool all = true, anybad = false, capped = false;
     for (int l = 0; l < loads; ++l) {
       const double thr = std::sqrt(h[l].target2);
@@ -373,7 +379,66 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
     all = all && ok[l];
   }
   c->last_refinements = 1;
+  c->last_launches = launches;
   return all ? PGJ_OK : PGJ_ERR_CERTIFICATION;
+}
+
+long long pgj_last_launches(pgj_ctx* c) { return c ? c->last_launches : -1; }
+
+int pgj_profile_iteration(pgj_ctx* c, int loads, const double* macros, int reps, double* ms, double* bytes,
+                          void* stream) {
+  if (!c || !macros || !ms || !bytes || loads < 1 || loads > c->L || reps < 1 || c->prec != PGJ_FP64)
+    return PGJ_ERR_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t N = size_t(c->N), N3 = 3 * N, Nh = size_t(c->Nh);
+  int st = stage_macros(c, loads, macros, s);
+  if (!st) st = launch_rhs(c, loads, c->macros, c->f, s);
+  if (!st) st = launch_norms(c, loads, c->f, 1e-30, s);  // tiny target: loads stay active while timed
+  if (st) return st;
+  cudaError_t e = cudaMemsetAsync(c->x, 0, sizeof(double) * N3 * loads, s);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  if ((st = capture_cert(c, loads, s))) return st;
+  if ((st = launch_init_mask(c, loads, s))) return st;
+  if ((st = launch_green(c, loads, PGJ_FP64, c->r, true, s))) return st;
+  if ((st = launch_update_p(c, loads, PGJ_FP64, true, s, 0, false))) return st;
+  cudaEvent_t ev[2 * PGJ_PROFILE_KERNELS];
+  for (int k = 0; k < 2 * PGJ_PROFILE_KERNELS; ++k) cudaEventCreate(&ev[k]);
+  double acc[PGJ_PROFILE_KERNELS] = {0};
+  for (int rep = 0; rep < reps && !st; ++rep) {
+    for (int k = 0; k < PGJ_PROFILE_KERNELS && !st; ++k) {
+      cudaEventRecord(ev[2 * k], s);
+      if (k == 0) st = launch_stencil(c, kPCG, loads, PGJ_FP64, c->p, c->q, nullptr, nullptr, s);
+      else if (k == 1) st = launch_update_ur(c, loads, PGJ_FP64, c->x, nullptr, s);
+      else if (k < 7) st = launch_green_pass(c, loads, PGJ_FP64, c->r, false, k - 2, s);
+      else st = launch_update_p(c, loads, PGJ_FP64, false, s, 0, false);
+      cudaEventRecord(ev[2 * k + 1], s);
+    }
+    if (!st && (e = cudaStreamSynchronize(s)) != cudaSuccess) st = set_cuda_error(e);
+    for (int k = 0; k < PGJ_PROFILE_KERNELS && !st; ++k) {
+      float t = 0.f;
+      cudaEventElapsedTime(&t, ev[2 * k], ev[2 * k + 1]);
+      acc[k] += t;
+    }
+  }
+  for (int k = 0; k < 2 * PGJ_PROFILE_KERNELS; ++k) cudaEventDestroy(ev[k]);
+  if (st) return st;
+  const double V = double(N3) * 8.0 * loads;          // one FP64 DOF vector over all loads
+  const double S = double(Nh) * 3 * 16.0 * loads;     // one complex half spectrum over all loads
+  const double sc = double(N3) * 8.0;                 // scale field
+  const double algo[PGJ_PROFILE_KERNELS] = {
+      2 * V + 8.0 * N,                  // operator: read p (+a), write q
+      6 * V,                            // update_ur: read u p r q, write u r
+      V + sc + S,                       // fft_x: read r (+s), write spectrum
+      2 * S,                            // fft_y
+      2 * S + 6.0 * Nh * 8,             // fft_z: spectrum in/out + symbol
+      2 * S,                            // ifft_y
+      S + sc + V,                       // ifft_x: read spectrum (+s), write s.w
+      3 * V};                           // update_p: read s.w p, write p
+  for (int k = 0; k < PGJ_PROFILE_KERNELS; ++k) {
+    ms[k] = acc[k] / reps;
+    bytes[k] = algo[k];
+  }
+  return PGJ_OK;
 }
 
 int pgj_energies(pgj_ctx* c, int loads, const double* u, const double* macros, double* e, void* stream) {

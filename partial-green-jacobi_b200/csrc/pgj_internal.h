@@ -103,6 +103,7 @@ struct pgj_ctx {
   double alpha;
   double inner_rtol;
   int last_refinements;
+  long long last_launches;
   pgj::Graphs* graphs;
 };
 
@@ -120,6 +121,8 @@ int launch_norms(pgj_ctx* c, int loads, const double* f, double rtol, cudaStream
 int init_fft_tables(pgj_ctx* c, cudaStream_t s);
 int build_symbol(int n, double lam, double mu, double* sym, float* sym32, cudaStream_t s);
 int launch_green(pgj_ctx* c, int loads, int prec, const void* r, bool init, cudaStream_t s);
+// one Green pass: 0 fft_x, 1 fft_y, 2 fft_z+symbol, 3 ifft_y, 4 ifft_x
+int launch_green_pass(pgj_ctx* c, int loads, int prec, const void* r, bool init, int pass, cudaStream_t s);
 int launch_green_standalone(pgj_ctx* c, int loads, const double* r, double* z, cudaStream_t s);
 // pcg (pgj_pcg.cu)
 int launch_update_ur(pgj_ctx* c, int loads, int prec, double* u64, void* uT, cudaStream_t s);

@@ -202,6 +202,19 @@ class Operator:
     def last_refinements(self) -> int:
         return int(_lib.lib().pgj_last_refinements(self._ctx))
 
+    def last_launches(self) -> int:
+        return int(_lib.lib().pgj_last_launches(self._ctx))
+
+    def profile_iteration(self, macros, reps: int = 20):
+        """Per-kernel mean durations (ms) and algorithmic bytes of one PCG iteration (CUDA events)."""
+        m = np.ascontiguousarray(np.atleast_2d(np.asarray(macros, dtype=np.float64)))
+        ms = (C.c_double * 8)()
+        nbytes = (C.c_double * 8)()
+        _lib.check(_lib.lib().pgj_profile_iteration(self._ctx, m.shape[0], m.ctypes.data, int(reps), ms, nbytes,
+                                                    _stream_ptr()), "pgj_profile_iteration")
+        names = ["operator", "update_ur", "fft_x", "fft_y", "fft_z_symbol", "ifft_y", "ifft_x", "update_p"]
+        return {k: dict(ms=ms[i], bytes=nbytes[i]) for i, k in enumerate(names)}
+
     def energies(self, u, macros):
         torch = _torch()
         m = np.ascontiguousarray(np.atleast_2d(np.asarray(macros, dtype=np.float64)))
