@@ -78,16 +78,32 @@ __device__ __forceinline__ bool last_block(int* ticket, int nblocks) {
   return amlast;
 }
 
-// Block-wide sum of NV doubles; result valid in thread 0. Uses `red` (>= NV * 32 doubles).
+// Sum over the lanes of a warp that may be partial (the last warp of a block whose size is not a
+// multiple of 32): `active` lanes take part, lane 0 receives the sum.
+__device__ __forceinline__ double warp_reduce(double v, int lane, int active) {
+  if (active >= 32) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  } else {
+    const unsigned mask = (1u << active) - 1u;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double t = __shfl_down_sync(mask, v, o);
+      if (lane + o < active) v += t;
+    }
+  }
+  return v;
+}
+
+// Block-wide sum of NV doubles for any block size; result valid in thread 0. Uses `red`
+// (>= NV * 32 doubles).
 template <int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double* red) {
   const int tid = threadIdx.x + blockDim.x * threadIdx.y;
   const int nthreads = blockDim.x * blockDim.y;
-#pragma unroll
-  for (int k = 0; k < NV; ++k)
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_down_sync(0xffffffffu, v[k], o);
   const int warp = tid >> 5, lane = tid & 31, nwarps = (nthreads + 31) >> 5;
+  const int active = min(32, nthreads - (warp << 5));
+#pragma unroll
+  for (int k = 0; k < NV; ++k) v[k] = warp_reduce(v[k], lane, active);
   __syncthreads();
   if (lane == 0)
 #pragma unroll
@@ -97,21 +113,19 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* red) {
 #pragma unroll
     for (int k = 0; k < NV; ++k) {
       double s = lane < nwarps ? red[k * 32 + lane] : 0.0;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-      v[k] = s;
+      v[k] = warp_reduce(s, lane, active);
     }
   }
 }
 
-// Fixed-order sum of `count` partials (strided by 1) by one warp; result in lane 0.
+// Fixed-order sum of `count` partials by the first warp of the block (which may be partial);
+// call from every thread with tid < 32; result in thread 0.
 __device__ __forceinline__ double warp_sum_partials(const double* p, int count) {
-  const int lane = threadIdx.x & 31;
+  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+  const int active = min(32, int(blockDim.x * blockDim.y));
   double s = 0.0;
-  for (int i = lane; i < count; i += 32) s += __ldcg(p + i);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-  return s;
+  for (int i = tid; i < count; i += active) s += __ldcg(p + i);
+  return warp_reduce(s, tid, active);
 }
 
 // --------------------------------------------------------------------------- operator constants
