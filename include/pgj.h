@@ -141,6 +141,18 @@ int pgj_energies(pgj_ctx* ctx, int loads, const double* u, const double* macros,
  * float64 to device `C` (PaperResident.effective_tensor, reproduction.py:166-176). */
 int pgj_effective_tensor(pgj_ctx* ctx, const double* u, double* C, void* stream);
 
+/* Homogenized tensor of six Voigt solutions without any device allocation (no counterpart in the
+ * reference). For callers that cannot allocate device memory: a host application that owns the
+ * device memory pool and forbids third-party allocations, or code running while a CUDA graph is
+ * captured, where cudaMalloc cannot be recorded. The caller passes a (n^3), u (6, 3N) and C (36
+ * float64), all device; the scratch lives in a fixed file-scope device array of about 0.69 MB per
+ * GPU, held until exit. Accepts 2 <= n <= 256 (PGJ_ERR_ARGUMENT otherwise). The first call on a
+ * device looks up the array's device address and writes its constants (a synchronous copy), so
+ * make that first call before any stream capture. All calls share the array: calls that overlap on
+ * the GPU race and must be ordered on one stream. */
+int pgj_effective_tensor_noalloc(int n, double lam, double mu, const double* a, const double* u, double* C,
+                                 void* stream);
+
 /* ------------------------------------------------------------------ design update (OC)
  * Study II (paper) chain: clipped cone filter, tanh(beta, eta) projection and damped OC with the
  * MATLAB bisection stop (PaperOuter, exp/asg_sctop_reproduction_20261105/reproduction.py:69-118,

@@ -65,6 +65,7 @@ SIGNATURES = {
     "pgj_profile_iteration": (C.c_int, [vp, C.c_int, vp, C.c_int, vp, vp, vp]),
     "pgj_energies": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
     "pgj_effective_tensor": (C.c_int, [vp, vp, vp, vp]),
+    "pgj_effective_tensor_noalloc": (C.c_int, [C.c_int, f64, f64, vp, vp, vp, vp]),
     "pgj_cone_filter": (C.c_int, [C.c_int, vp, vp, C.c_int, vp, vp, vp]),
     "pgj_paper_project": (C.c_int, [C.c_int, vp, vp, f64, f64, f64, vp, vp, vp, vp]),
     "pgj_paper_oc": (C.c_int, [C.c_int, vp, vp, C.c_int, vp, vp, vp, vp, vp, f64, f64, f64, f64, f64, f64, f64,

@@ -163,3 +163,90 @@ int launch_effective_tensor(pgj_ctx* c, const double* u, double* C, double* e, c
 }
 
 }  // namespace pgj
+
+// ------------------------------------------------------------------------------------------------
+// Homogenized tensor without any device allocation by the caller or the library.
+//
+// Some callers cannot allocate device memory: a host application that owns the whole device
+// memory pool and forbids third-party cudaMalloc (for instance a finite-element code that calls
+// this library as a post-processing plugin inside its own memory budget), or code that has to
+// run while a CUDA graph is being captured, where cudaMalloc is not a capturable operation. They
+// still hold the density field and the six solutions, and want C_H from them. This entry point
+// runs the same C_H kernel as pgj_effective_tensor, with its scratch (block partial sums, the
+// last-block ticket and the six unit Voigt strains) in a fixed file-scope device array instead of
+// a context workspace.
+//
+// Limits and sharing: the array is kNoAllocScratchBytes (about 0.69 MB) on every GPU that loads
+// the library, held until the process exits; it fits the kernel's partial sums for any grid the
+// entry point accepts (2 <= n <= 256). Every call on a device uses the same array and the array
+// keeps the last call's contents; the ticket is cleared at the start of each call. Two calls whose
+// work overlaps on the GPU (for example on two streams without ordering) race on the array and
+// give wrong results: order them on one stream or synchronise between them.
+namespace {
+constexpr size_t kNoAllocPartialDoubles = size_t(21) * pgj::kMaxPartials;
+constexpr size_t kNoAllocVoigtDoubles = 64;
+constexpr size_t kNoAllocScalarBytes = 256;
+constexpr size_t kNoAllocScratchBytes =
+    kNoAllocPartialDoubles * sizeof(double) + kNoAllocVoigtDoubles * sizeof(double) + kNoAllocScalarBytes;
+static_assert(sizeof(pgj::LoadScalars) <= kNoAllocScalarBytes, "scalar record must fit its slot");
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+// Device address of g_noalloc_scratch per device ordinal, obtained once with that device current.
+// The host-side name g_noalloc_scratch is only a stand-in for the symbol and is never passed to
+// a kernel.
+unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {nullptr};
+
+int noalloc_setup(int device, unsigned char** out) {
+  if (g_noalloc_addr[device]) {
+    *out = g_noalloc_addr[device];
+    return PGJ_OK;
+  }
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess) return pgj::set_cuda_error(e);
+  unsigned char* base = static_cast<unsigned char*>(p);
+  double eye[36] = {0};
+  for (int i = 0; i < 6; ++i) eye[i * 6 + i] = 1.0;
+  // synchronous copy: done once per device, before any stream capture by contract
+  e = cudaMemcpy(base + kNoAllocPartialDoubles * sizeof(double), eye, sizeof(eye), cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) return pgj::set_cuda_error(e);
+  g_noalloc_addr[device] = base;
+  *out = base;
+  return PGJ_OK;
+}
+}  // namespace
+
+extern "C" int pgj_effective_tensor_noalloc(int n, double lam, double mu, const double* a, const double* u,
+                                            double* C, void* stream) {
+  if (n < 2 || n > 256) return PGJ_ERR_ARGUMENT;  // beyond the grids this scratch is sized for
+  if (!a || !u || !C || !(mu > 0) || !(lam + 2 * mu / 3 > 0)) return PGJ_ERR_ARGUMENT;
+  int device = 0;
+  cudaError_t e = cudaGetDevice(&device);
+  if (e != cudaSuccess) return pgj::set_cuda_error(e);
+  if (device < 0 || device >= kNoAllocMaxDevices) return PGJ_ERR_UNSUPPORTED;
+  unsigned char* base = nullptr;
+  int st = noalloc_setup(device, &base);
+  if (st) return st;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  double* partials = reinterpret_cast<double*>(base);
+  double* voigt = partials + kNoAllocPartialDoubles;
+  pgj::LoadScalars* scal = reinterpret_cast<pgj::LoadScalars*>(voigt + kNoAllocVoigtDoubles);
+  // the last-block ticket must start at zero
+  e = cudaMemsetAsync(scal, 0, sizeof(pgj::LoadScalars), s);
+  if (e != cudaSuccess) return pgj::set_cuda_error(e);
+  pgj::EnergyArgs A;
+  A.n = n; A.loads = 6; A.u = u; A.macros = voigt; A.a = a;
+  A.e = nullptr; A.C = C; A.scal = scal; A.partials = partials;
+  A.kc = pgj::make_opconst(n, lam, mu);
+  const size_t N = size_t(n) * n * n;
+  unsigned blocks = 4 * 148;
+  const unsigned need = unsigned((N + pgj::kEnergyThreads - 1) / pgj::kEnergyThreads);
+  if (blocks > need) blocks = need;
+  const size_t smem = size_t(6) * 21 * pgj::kEnergyThreads * sizeof(double);
+  e = cudaFuncSetAttribute(pgj::k_energy<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
+  if (e != cudaSuccess) return pgj::set_cuda_error(e);
+  pgj::k_energy<true><<<blocks, pgj::kEnergyThreads, smem, s>>>(A);
+  return pgj::check_launch();
+}
