@@ -57,6 +57,8 @@ struct LoadScalars {
   int bad;          // non-finite / non-positive curvature latch
   int failed;       // set by the apply finalizer when p.q or rz is invalid
   int iterations;   // PCG iterations taken
+  int touched;      // mixed refinement: this load ran an inner solve in the current sweep
+  int total_iterations;  // mixed refinement: inner iterations summed over sweeps
   int ticket[8];    // per-kernel block tickets for the last-block finalizers
 };
 

@@ -24,8 +24,9 @@ int set_cuda_error(cudaError_t e) {
 struct Graphs {
   cudaStream_t cap = nullptr;  // private capture stream
   int loads = 0;
+  double inner_rtol = 0.0;
   cudaGraphExec_t cert = nullptr;
-  cudaGraphExec_t attempt = nullptr;
+  cudaGraphExec_t attempt = nullptr;  // FP64: init + PCG loop + certify; mixed: one refinement sweep
   ~Graphs() {
     if (cert) cudaGraphExecDestroy(cert);
     if (attempt) cudaGraphExecDestroy(attempt);
@@ -57,6 +58,7 @@ static Layout make_layout(int n, int L, int prec) {
   y.f = take(sizeof(double) * N3 * L);
   y.x = take(sizeof(double) * N3 * L);
   y.r64 = take(prec == PGJ_FP32 ? sizeof(double) * N3 * L : 0);
+  y.d = take(prec == PGJ_FP32 ? tsz * N3 * L : 0);
   y.r = take(tsz * N3 * L);
   y.p = take(tsz * N3 * L);
   y.q = take(tsz * N3 * L);
@@ -67,18 +69,28 @@ static Layout make_layout(int n, int L, int prec) {
 }
 
 // ------------------------------------------------------------------------------------ graphs
+// certification: u <- P u, r = f - K u (FP64), ||r||, mean r (resident.py:133-136)
 static int capture_cert(pgj_ctx* c, int L, cudaStream_t s) {
   int st = launch_project_u(c, L, c->x, s);
   if (st) return st;
-  return launch_stencil(c, kResidual, L, PGJ_FP64, c->x, c->r, c->f, nullptr, s);
+  double* r = c->prec == PGJ_FP32 ? c->r64 : static_cast<double*>(c->r);
+  LoadScalars* saved = c->scal;
+  c->scal = c->scal_out;
+  st = launch_stencil(c, kResidual, L, PGJ_FP64, c->x, r, c->f, nullptr, s);
+  c->scal = saved;
+  return st;
 }
 
+// one PCG iteration in the inner precision (resident.py:125-131)
 static int capture_iteration(pgj_ctx* c, int L, cudaStream_t s, cudaGraphConditionalHandle h, bool last) {
+  const int prec = c->prec;
   int st;
-  if ((st = launch_stencil(c, kPCG, L, PGJ_FP64, c->p, c->q, nullptr, nullptr, s))) return st;
-  if ((st = launch_update_ur(c, L, PGJ_FP64, c->x, nullptr, s))) return st;
-  if ((st = launch_green(c, L, PGJ_FP64, c->r, false, s))) return st;
-  return launch_update_p(c, L, PGJ_FP64, false, s, h, last);
+  if ((st = launch_stencil(c, kPCG, L, prec, c->p, c->q, nullptr, nullptr, s))) return st;
+  if (prec == PGJ_FP32) st = launch_update_ur(c, L, prec, nullptr, c->d, s);
+  else st = launch_update_ur(c, L, prec, c->x, nullptr, s);
+  if (st) return st;
+  if ((st = launch_green(c, L, prec, c->r, false, s))) return st;
+  return launch_update_p(c, L, prec, false, s, h, last);
 }
 
 static int end_capture(cudaStream_t s, cudaGraph_t* g, int st) {
@@ -88,9 +100,46 @@ static int end_capture(cudaStream_t s, cudaGraph_t* g, int st) {
   return PGJ_OK;
 }
 
+// Appends to the capture on `s`: directions init, then WHILE(any load active){iteration}.
+static int capture_pcg(pgj_ctx* c, int L, cudaStream_t s) {
+  int st = launch_green(c, L, c->prec, c->r, true, s);
+  if (!st) st = launch_update_p(c, L, c->prec, true, s, 0, false);
+  if (st) return st;
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &ndeps);
+  cudaGraphConditionalHandle h = 0;
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, cg, deps, ndeps, &cp);
+  if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaStream_t s2;
+  e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  e = cudaStreamBeginCaptureToGraph(s2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    st = set_cuda_error(e);
+  } else {
+    st = capture_iteration(c, L, s2, h, true);
+    cudaGraph_t bg = body;
+    cudaError_t e2 = cudaStreamEndCapture(s2, &bg);
+    if (!st && e2 != cudaSuccess) st = set_cuda_error(e2);
+  }
+  cudaStreamDestroy(s2);
+  return st;
+}
+
 static int build_graphs(pgj_ctx* c, int L) {
   Graphs* G = c->graphs;
-  if (G->loads == L && G->cert && G->attempt) return PGJ_OK;
+  if (G->loads == L && G->cert && G->attempt && G->inner_rtol == c->inner_rtol) return PGJ_OK;
   if (G->cert) { cudaGraphExecDestroy(G->cert); G->cert = nullptr; }
   if (G->attempt) { cudaGraphExecDestroy(G->attempt); G->attempt = nullptr; }
   cudaStream_t s = G->cap;
@@ -104,43 +153,20 @@ static int build_graphs(pgj_ctx* c, int L) {
   e = cudaGraphInstantiate(&G->cert, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return set_cuda_error(e);
-  // attempt graph: init -> while(any active){iteration} -> certify
+  // FP64 attempt: init masks -> PCG loop -> certify.
+  // Mixed sweep: r_in = T(r64), d = 0 -> inner PCG loop (FP32) -> x += d -> FP64 certify.
   if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return set_cuda_error(e);
-  st = launch_init_mask(c, L, s);
-  if (!st) st = launch_green(c, L, PGJ_FP64, c->r, true, s);
-  if (!st) st = launch_update_p(c, L, PGJ_FP64, true, s, 0, false);
-  cudaGraphNode_t node = nullptr;
-  if (!st) {
-    cudaStreamCaptureStatus cs;
-    cudaGraph_t cg = nullptr;
-    const cudaGraphNode_t* deps = nullptr;
-    size_t ndeps = 0;
-    e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &ndeps);
-    cudaGraphConditionalHandle h = 0;
-    if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, cg, 1, cudaGraphCondAssignDefault);
-    cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
-    cp.conditional.handle = h;
-    cp.conditional.type = cudaGraphCondTypeWhile;
-    cp.conditional.size = 1;
-    if (e == cudaSuccess) e = cudaGraphAddNode(&node, cg, deps, ndeps, &cp);
-    if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
-    if (e != cudaSuccess) {
-      st = set_cuda_error(e);
-    } else {
-      cudaGraph_t body = cp.conditional.phGraph_out[0];
-      cudaStream_t s2;
-      e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
-      if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(s2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
-      if (e != cudaSuccess) {
-        st = set_cuda_error(e);
-      } else {
-        st = capture_iteration(c, L, s2, h, true);
-        cudaGraph_t bg = body;
-        cudaError_t e2 = cudaStreamEndCapture(s2, &bg);
-        if (!st && e2 != cudaSuccess) st = set_cuda_error(e2);
-      }
-      cudaStreamDestroy(s2);
+  if (c->prec == PGJ_FP32) {
+    st = launch_inner_start(c, L, c->inner_rtol, s);
+    if (!st) {
+      c->scal = c->scal_in;
+      st = capture_pcg(c, L, s);
+      c->scal = c->scal_out;
     }
+    if (!st) st = launch_inner_finish(c, L, s);
+  } else {
+    st = launch_init_mask(c, L, s);
+    if (!st) st = capture_pcg(c, L, s);
   }
   if (!st) st = capture_cert(c, L, s);
   if ((st = end_capture(s, &g, st))) return st;
@@ -148,6 +174,7 @@ static int build_graphs(pgj_ctx* c, int L) {
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return set_cuda_error(e);
   G->loads = L;
+  G->inner_rtol = c->inner_rtol;
   return PGJ_OK;
 }
 
@@ -205,7 +232,7 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
   c->kc = make_opconst(n, lam, mu);
   make_fft_plan(n, &c->plan);
   c->sg = stencil_geom(n, loads);
-  c->fg = fft_geom(n, precision == PGJ_FP32 ? 4 : 8);
+  c->fg = fft_geom(n, precision == PGJ_FP32 ? 4 : 8, c->plan);
   c->lay = y;
   c->base = static_cast<char*>(workspace);
   c->bytes = workspace_bytes;
@@ -221,7 +248,10 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
   c->r64 = precision == PGJ_FP32 ? reinterpret_cast<double*>(b + y.r64) : nullptr;
   c->r = b + y.r; c->p = b + y.p; c->q = b + y.q; c->sw = b + y.sw; c->spec = b + y.spec;
   c->partials = reinterpret_cast<double*>(b + y.partials);
-  c->scal = reinterpret_cast<LoadScalars*>(b + y.scal);
+  c->scal_out = reinterpret_cast<LoadScalars*>(b + y.scal);
+  c->scal_in = c->scal_out + loads;
+  c->scal = c->scal_out;
+  c->d = precision == PGJ_FP32 ? static_cast<void*>(b + y.d) : nullptr;
   c->macros = reinterpret_cast<double*>(b + y.macros);
   c->cond = reinterpret_cast<int*>(b + y.cond);
   c->aux = reinterpret_cast<double*>(b + y.aux);
@@ -323,11 +353,16 @@ int pgj_set_inner_rtol(pgj_ctx* c, double inner_rtol) {
 
 int pgj_last_refinements(pgj_ctx* c) { return c ? c->last_refinements : -1; }
 
+// Maximum FP64 refinement sweeps of the mixed solve (each sweep: one FP32 inner PCG solve to
+// inner_rtol relative, x += d, FP64 certification).
+static constexpr int kMaxSweeps = 12;
+
 int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* u, pgj_load_info* info, void* stream) {
   if (!c || !macros || !u || !info || loads < 1 || loads > c->L || !(rtol > 0)) return PGJ_ERR_ARGUMENT;
-  if (c->prec != PGJ_FP64) return PGJ_ERR_UNSUPPORTED;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const size_t N3 = 3 * size_t(c->N);
+  const bool mixed = c->prec == PGJ_FP32;
+  c->scal = c->scal_out;
   int st = stage_macros(c, loads, macros, s);
   if (!st) st = launch_rhs(c, loads, c->macros, c->f, s);
   if (!st) st = launch_norms(c, loads, c->f, rtol, s);
@@ -339,28 +374,53 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
   if ((e = cudaGraphLaunch(c->graphs->cert, s)) != cudaSuccess) return set_cuda_error(e);
   std::vector<LoadScalars> h(loads);
   std::vector<int> ok(loads, 0);
-  int restarts = 0;
+  int restarts = 0, sweeps = 0;
   int body[2] = {0, 0};
   long long launches = 2 + 3;  // rhs + norms, initial certification
-  for (;;) {
-    if ((e = cudaGraphLaunch(c->graphs->attempt, s)) != cudaSuccess) return set_cuda_error(e);
-    e = cudaMemcpyAsync(h.data(), c->scal, sizeof(LoadScalars) * loads, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(body, c->cond, sizeof(body), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-    if (e != cudaSuccess) return set_cuda_error(e);
-    // attempt: init mask + 5 Green passes + p init, 8 kernels per loop body, 3 certification kernels
-    launches += 7 + 8LL * body[0] + 3;
-    if (body[1]) return PGJ_ERR_ITERATION_CAP;
-    bool all = true, anybad = false, capped = false;
+  bool capped_by_bound = false;
+  auto read_state = [&](bool with_body) -> cudaError_t {
+    cudaError_t err = cudaMemcpyAsync(h.data(), c->scal_out, sizeof(LoadScalars) * loads, cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess && with_body) err = cudaMemcpyAsync(body, c->cond, sizeof(body), cudaMemcpyDeviceToHost, s);
+    if (err == cudaSuccess) err = cudaStreamSynchronize(s);
+    return err;
+  };
+  auto evaluate = [&](bool& all, bool& anybad, bool& capped) {
+    all = true; anybad = false; capped = false;
     for (int l = 0; l < loads; ++l) {
       const double thr = std::sqrt(h[l].target2);
       ok[l] = std::isfinite(h[l].absolute) && h[l].absolute <= thr && h[l].bad == 0;
       all = all && ok[l];
       anybad = anybad || h[l].bad;
-      capped = capped || (!ok[l] && h[l].iterations >= 4000);
+      const int its = mixed ? h[l].total_iterations : h[l].iterations;
+      capped = capped || (!ok[l] && its >= 4000);
     }
-    if (all || restarts >= 2 || anybad || capped) break;
-    ++restarts;
+  };
+  if (mixed) {
+    // one FP32 inner solve per sweep inside FP64 iterative refinement
+    if ((e = read_state(false)) != cudaSuccess) return set_cuda_error(e);
+    for (;;) {
+      bool all, anybad, capped;
+      evaluate(all, anybad, capped);
+      if (all || anybad || capped || sweeps >= kMaxSweeps) break;
+      if ((e = cudaGraphLaunch(c->graphs->attempt, s)) != cudaSuccess) return set_cuda_error(e);
+      ++sweeps;
+      if ((e = read_state(true)) != cudaSuccess) return set_cuda_error(e);
+      // sweep: inner start + 5 Green passes + p init, 8 kernels per loop body, x += d, 3 certification kernels
+      launches += 1 + 6 + 8LL * body[0] + 1 + 3;
+      if (body[1]) { capped_by_bound = true; break; }
+    }
+  } else {
+    for (;;) {
+      if ((e = cudaGraphLaunch(c->graphs->attempt, s)) != cudaSuccess) return set_cuda_error(e);
+      if ((e = read_state(true)) != cudaSuccess) return set_cuda_error(e);
+      // attempt: init mask + 5 Green passes + p init, 8 kernels per loop body, 3 certification kernels
+      launches += 7 + 8LL * body[0] + 3;
+      if (body[1]) { capped_by_bound = true; break; }
+      bool all, anybad, capped;
+      evaluate(all, anybad, capped);
+      if (all || restarts >= 2 || anybad || capped) break;
+      ++restarts;
+    }
   }
   if (u != c->x) e = cudaMemcpyAsync(u, c->x, sizeof(double) * N3 * loads, cudaMemcpyDeviceToDevice, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -368,18 +428,21 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
   bool all = true;
   for (int l = 0; l < loads; ++l) {
     pgj_load_info& I = info[l];
+    const double thr = std::sqrt(h[l].target2);
+    ok[l] = std::isfinite(h[l].absolute) && h[l].absolute <= thr && h[l].bad == 0;
     I.rhs_norm = h[l].norm;
     I.absolute_residual = h[l].absolute;
-    I.threshold = std::sqrt(h[l].target2);
+    I.threshold = thr;
     I.relative_residual = h[l].absolute / (h[l].norm > 1e-300 ? h[l].norm : 1e-300);
-    I.iterations = h[l].iterations;
+    I.iterations = mixed ? h[l].total_iterations : h[l].iterations;
     I.converged = ok[l];
     I.restarts = restarts;
     I.bad = h[l].bad;
     all = all && ok[l];
   }
-  c->last_refinements = 1;
+  c->last_refinements = mixed ? sweeps : 1;
   c->last_launches = launches;
+  if (capped_by_bound) return PGJ_ERR_ITERATION_CAP;
   return all ? PGJ_OK : PGJ_ERR_CERTIFICATION;
 }
 
@@ -387,10 +450,11 @@ long long pgj_last_launches(pgj_ctx* c) { return c ? c->last_launches : -1; }
 
 int pgj_profile_iteration(pgj_ctx* c, int loads, const double* macros, int reps, double* ms, double* bytes,
                           void* stream) {
-  if (!c || !macros || !ms || !bytes || loads < 1 || loads > c->L || reps < 1 || c->prec != PGJ_FP64)
-    return PGJ_ERR_ARGUMENT;
+  if (!c || !macros || !ms || !bytes || loads < 1 || loads > c->L || reps < 1) return PGJ_ERR_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const size_t N = size_t(c->N), N3 = 3 * N, Nh = size_t(c->Nh);
+  const int prec = c->prec;
+  c->scal = c->scal_out;
   int st = stage_macros(c, loads, macros, s);
   if (!st) st = launch_rhs(c, loads, c->macros, c->f, s);
   if (!st) st = launch_norms(c, loads, c->f, 1e-30, s);  // tiny target: loads stay active while timed
@@ -398,19 +462,25 @@ int pgj_profile_iteration(pgj_ctx* c, int loads, const double* macros, int reps,
   cudaError_t e = cudaMemsetAsync(c->x, 0, sizeof(double) * N3 * loads, s);
   if (e != cudaSuccess) return set_cuda_error(e);
   if ((st = capture_cert(c, loads, s))) return st;
-  if ((st = launch_init_mask(c, loads, s))) return st;
-  if ((st = launch_green(c, loads, PGJ_FP64, c->r, true, s))) return st;
-  if ((st = launch_update_p(c, loads, PGJ_FP64, true, s, 0, false))) return st;
+  if (prec == PGJ_FP32) {
+    if ((st = launch_inner_start(c, loads, c->inner_rtol, s))) return st;
+    c->scal = c->scal_in;
+  } else if ((st = launch_init_mask(c, loads, s))) {
+    return st;
+  }
+  if (!st) st = launch_green(c, loads, prec, c->r, true, s);
+  if (!st) st = launch_update_p(c, loads, prec, true, s, 0, false);
   cudaEvent_t ev[2 * PGJ_PROFILE_KERNELS];
   for (int k = 0; k < 2 * PGJ_PROFILE_KERNELS; ++k) cudaEventCreate(&ev[k]);
   double acc[PGJ_PROFILE_KERNELS] = {0};
   for (int rep = 0; rep < reps && !st; ++rep) {
     for (int k = 0; k < PGJ_PROFILE_KERNELS && !st; ++k) {
       cudaEventRecord(ev[2 * k], s);
-      if (k == 0) st = launch_stencil(c, kPCG, loads, PGJ_FP64, c->p, c->q, nullptr, nullptr, s);
-      else if (k == 1) st = launch_update_ur(c, loads, PGJ_FP64, c->x, nullptr, s);
-      else if (k < 7) st = launch_green_pass(c, loads, PGJ_FP64, c->r, false, k - 2, s);
-      else st = launch_update_p(c, loads, PGJ_FP64, false, s, 0, false);
+      if (k == 0) st = launch_stencil(c, kPCG, loads, prec, c->p, c->q, nullptr, nullptr, s);
+      else if (k == 1) st = prec == PGJ_FP32 ? launch_update_ur(c, loads, prec, nullptr, c->d, s)
+                                             : launch_update_ur(c, loads, prec, c->x, nullptr, s);
+      else if (k < 7) st = launch_green_pass(c, loads, prec, c->r, false, k - 2, s);
+      else st = launch_update_p(c, loads, prec, false, s, 0, false);
       cudaEventRecord(ev[2 * k + 1], s);
     }
     if (!st && (e = cudaStreamSynchronize(s)) != cudaSuccess) st = set_cuda_error(e);
@@ -420,17 +490,19 @@ int pgj_profile_iteration(pgj_ctx* c, int loads, const double* macros, int reps,
       acc[k] += t;
     }
   }
+  c->scal = c->scal_out;
   for (int k = 0; k < 2 * PGJ_PROFILE_KERNELS; ++k) cudaEventDestroy(ev[k]);
   if (st) return st;
-  const double V = double(N3) * 8.0 * loads;          // one FP64 DOF vector over all loads
-  const double S = double(Nh) * 3 * 16.0 * loads;     // one complex half spectrum over all loads
-  const double sc = double(N3) * 8.0;                 // scale field
+  const double sz = prec == PGJ_FP32 ? 4.0 : 8.0;     // bytes per real of the inner precision
+  const double V = double(N3) * sz * loads;           // one DOF vector over all loads
+  const double S = double(Nh) * 3 * 2 * sz * loads;  // one complex half spectrum over all loads
+  const double sc = double(N3) * 8.0;                 // scale field (FP64)
   const double algo[PGJ_PROFILE_KERNELS] = {
       2 * V + 8.0 * N,                  // operator: read p (+a), write q
       6 * V,                            // update_ur: read u p r q, write u r
       V + sc + S,                       // fft_x: read r (+s), write spectrum
       2 * S,                            // fft_y
-      2 * S + 6.0 * Nh * 8,             // fft_z: spectrum in/out + symbol
+      2 * S + 6.0 * Nh * sz,            // fft_z: spectrum in/out + symbol
       2 * S,                            // ifft_y
       S + sc + V,                       // ifft_x: read spectrum (+s), write s.w
       3 * V};                           // update_p: read s.w p, write p

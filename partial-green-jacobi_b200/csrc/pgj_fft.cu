@@ -34,7 +34,7 @@ bool make_fft_plan(int n, FFTPlan* plan) {
 // smem budget per block for the line buffers (two ping-pong buffers)
 static constexpr size_t kFFTSmemBudget = 200 * 1024;
 
-FFTGeom fft_geom(int n, int elem_bytes) {
+FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan) {
   FFTGeom g;
   const size_t cb = 2 * size_t(elem_bytes);  // complex bytes
   const size_t line = size_t(n + 1) * cb;
@@ -55,6 +55,17 @@ FFTGeom fft_geom(int n, int elem_bytes) {
   kcz = (ns + nkz - 1) / nkz;
   g.kcz = kcz;
   g.nkz = nkz;
+  // threads: enough for every butterfly of the widest stage, a multiple of 32, at most 512
+  int minr = 8;
+  for (int i = 0; i < plan.nst; ++i) minr = plan.radix[i] < minr ? plan.radix[i] : minr;
+  auto threads = [&](int lines) {
+    int t = lines * (n / minr);
+    t = (t + 31) / 32 * 32;
+    return t < 64 ? 64 : (t > 512 ? 512 : t);
+  };
+  g.thr_x = threads(3 * g.rb / 2);
+  g.thr_y = threads(g.kcy);
+  g.thr_z = threads(3 * g.kcz);
   return g;
 }
 
@@ -212,7 +223,7 @@ __device__ __forceinline__ bool load_on(const GreenArgs& A, int load) {
 
 // ---------------------------------------------------------------------------- FX
 template <typename T>
-__global__ void __launch_bounds__(256) k_fx(const GreenArgs A) {
+__global__ void __launch_bounds__(512) k_fx(const GreenArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int load = blockIdx.y;
@@ -264,7 +275,7 @@ __global__ void __launch_bounds__(256) k_fx(const GreenArgs A) {
 
 // ---------------------------------------------------------------------------- FY / IFY
 template <typename T, bool INV>
-__global__ void __launch_bounds__(256) k_fy(const GreenArgs A) {
+__global__ void __launch_bounds__(512) k_fy(const GreenArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int lc = blockIdx.z;  // load * 3 + component
@@ -294,7 +305,7 @@ __global__ void __launch_bounds__(256) k_fy(const GreenArgs A) {
 
 // ---------------------------------------------------------------------------- FZ (+ symbol)
 template <typename T>
-__global__ void __launch_bounds__(256) k_fz(const GreenArgs A) {
+__global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int load = blockIdx.z;
@@ -372,7 +383,7 @@ __global__ void __launch_bounds__(256) k_fz(const GreenArgs A) {
 
 // ---------------------------------------------------------------------------- IFX
 template <typename T>
-__global__ void __launch_bounds__(256) k_ifx(const GreenArgs A) {
+__global__ void __launch_bounds__(512) k_ifx(const GreenArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int load = blockIdx.y;
@@ -474,32 +485,22 @@ static int run_green_pass(pgj_ctx* c, int loads, GreenArgs& A, cudaStream_t s, i
   const int n = c->n;
   const FFTGeom& g = c->fg;
   switch (pass) {
-    case 0: k_fx<T><<<dim3((n * n) / g.rb, loads), 256, smem_x(c, cb), s>>>(A); break;
-    case 1: k_fy<T, false><<<dim3(g.nky, n, 3 * loads), 256, smem_y(c, cb), s>>>(A); break;
-    case 2: k_fz<T><<<dim3(g.nkz, n, loads), 256, smem_z(c, cb), s>>>(A); break;
-    case 3: k_fy<T, true><<<dim3(g.nky, n, 3 * loads), 256, smem_y(c, cb), s>>>(A); break;
-    default: k_ifx<T><<<dim3((n * n) / g.rb, loads), 256, smem_x(c, cb), s>>>(A); break;
+    case 0: k_fx<T><<<dim3((n * n) / g.rb, loads), g.thr_x, smem_x(c, cb), s>>>(A); break;
+    case 1: k_fy<T, false><<<dim3(g.nky, n, 3 * loads), g.thr_y, smem_y(c, cb), s>>>(A); break;
+    case 2: k_fz<T><<<dim3(g.nkz, n, loads), g.thr_z, smem_z(c, cb), s>>>(A); break;
+    case 3: k_fy<T, true><<<dim3(g.nky, n, 3 * loads), g.thr_y, smem_y(c, cb), s>>>(A); break;
+    default: k_ifx<T><<<dim3((n * n) / g.rb, loads), g.thr_x, smem_x(c, cb), s>>>(A); break;
   }
   return check_launch();
 }
 
 template <typename T>
 static int run_green(pgj_ctx* c, int loads, GreenArgs& A, cudaStream_t s) {
-  int st;
-  const size_t cb = 2 * sizeof(T);
-  const int n = c->n, ns = c->ns;
-  const FFTGeom& g = c->fg;
-  k_fx<T><<<dim3((n * n) / g.rb, loads), 256, smem_x(c, cb), s>>>(A);
-  if ((st = check_launch())) return st;
-  k_fy<T, false><<<dim3(g.nky, n, 3 * loads), 256, smem_y(c, cb), s>>>(A);
-  if ((st = check_launch())) return st;
-  k_fz<T><<<dim3(g.nkz, n, loads), 256, smem_z(c, cb), s>>>(A);
-  if ((st = check_launch())) return st;
-  k_fy<T, true><<<dim3(g.nky, n, 3 * loads), 256, smem_y(c, cb), s>>>(A);
-  if ((st = check_launch())) return st;
-  k_ifx<T><<<dim3((n * n) / g.rb, loads), 256, smem_x(c, cb), s>>>(A);
-  (void)ns;
-  return check_launch();
+  for (int pass = 0; pass < 5; ++pass) {
+    const int st = run_green_pass<T>(c, loads, A, s, pass);
+    if (st) return st;
+  }
+  return PGJ_OK;
 }
 
 static GreenArgs green_args(pgj_ctx* c, int prec, const void* r) {

@@ -31,8 +31,9 @@ struct FFTGeom {
   int nky;       // y-pass chunks
   int kcz;       // kx columns per z-pass block
   int nkz;       // z-pass chunks
+  int thr_x, thr_y, thr_z;  // threads per block of the x, y and z passes (>= butterflies of a stage)
 };
-FFTGeom fft_geom(int n, int elem_bytes);
+FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan);
 
 enum StencilMode { kPlain = 0, kPCG = 1, kResidual = 2 };
 
@@ -60,7 +61,7 @@ constexpr int kAuxDoubles = kAuxPartials + kMaxPartials;
 
 struct Layout {
   size_t a, scale, symbol, symbol32, tw, solutions, f, x, r, p, q, sw, spec, partials, scal, macros,
-      cond, r64, aux, total;
+      cond, r64, d, aux, total;
 };
 
 struct Graphs;
@@ -95,7 +96,10 @@ struct pgj_ctx {
   void* sw;            // (L, 3N) T  s . w (unprojected preconditioned residual)
   void* spec;          // (L, 3, n, n, ns) complex T
   double* partials;    // (L, kPartialQ * kMaxPartials)
-  pgj::LoadScalars* scal;  // L records
+  pgj::LoadScalars* scal;  // L records used by the kernels being launched (outer or inner)
+  pgj::LoadScalars* scal_out;  // certification / FP64 recurrence records
+  pgj::LoadScalars* scal_in;   // mixed refinement: inner FP32 recurrence records
+  void* d;             // mixed: (L, 3N) T inner correction
   double* macros;      // (L, 6) device copy
   int* cond;           // device flags (any active)
   double* r64;         // mixed: fp64 residual (L, 3N)
@@ -129,6 +133,10 @@ int launch_update_ur(pgj_ctx* c, int loads, int prec, double* u64, void* uT, cud
 int launch_update_p(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, cudaGraphConditionalHandle h,
                     bool set_cond);
 int launch_init_mask(pgj_ctx* c, int loads, cudaStream_t s);
+// mixed refinement (pgj_pcg.cu): inner residual r = T(r64), d = 0, inner targets and masks;
+// then x += d for the loads solved in this sweep
+int launch_inner_start(pgj_ctx* c, int loads, double inner_rtol, cudaStream_t s);
+int launch_inner_finish(pgj_ctx* c, int loads, cudaStream_t s);
 // energy (pgj_energy.cu)
 int launch_energies(pgj_ctx* c, int loads, const double* u, const double* macros_dev, double* e, cudaStream_t s);
 int launch_effective_tensor(pgj_ctx* c, const double* u, double* C, double* e, cudaStream_t s);

@@ -12,6 +12,7 @@
 // scatter in exp/asg_gpu_resident_20261103/scalar_fi.cu:14-36).
 #include "pgj_internal.h"
 #include <cmath>
+#include <cstdlib>
 
 namespace pgj {
 
@@ -40,12 +41,21 @@ StencilGeom stencil_geom(int n, int loads) {
     if (waste < best - 1e-12) { best = waste; best_ty = ty; }
   }
   g.ty = best_ty;
+  // tuning override (sweeps): PGJ_STENCIL_TY rows per tile, PGJ_STENCIL_ZC planes per chunk
+  if (const char* e = std::getenv("PGJ_STENCIL_TY")) {
+    const int v = std::atoi(e);
+    if (v >= 1 && v <= n && n * (v + 1) <= maxthreads) g.ty = v;
+  }
   g.ntiles = (n + g.ty - 1) / g.ty;
   // aim for >= ~2 blocks per SM across the launch, z chunks of at least 4 planes
   int want = (2 * 148 + loads * g.ntiles - 1) / (loads * g.ntiles);
   int maxchunks = n / 4 > 0 ? n / 4 : 1;
   int nch = want < 1 ? 1 : (want > maxchunks ? maxchunks : want);
   g.zc = (n + nch - 1) / nch;
+  if (const char* e = std::getenv("PGJ_STENCIL_ZC")) {
+    const int v = std::atoi(e);
+    if (v >= 1 && v <= n) g.zc = v;
+  }
   g.nchunks = (n + g.zc - 1) / g.zc;
   return g;
 }
@@ -367,6 +377,8 @@ __global__ void k_norms(int n, const double* __restrict__ f, double rtol, LoadSc
       S.norm = norm;
       S.target2 = t * t;
       S.iterations = 0;
+      S.total_iterations = 0;
+      S.touched = 0;
       S.bad = 0;
       S.failed = 0;
       S.active = 0;

@@ -10,10 +10,32 @@
 
 namespace pgj {
 
+// 48-byte chunks of a DOF vector: 6 doubles (2 nodes) or 12 floats (4 nodes), read as three
+// 16-byte vectors; a chunk starts on a node, so element j of a chunk is component j % 3.
+template <typename T> struct Chunk;
+template <> struct Chunk<double> { static constexpr int CH = 6; using V = double2; };
+template <> struct Chunk<float> { static constexpr int CH = 12; using V = float4; };
+
 template <typename T>
-__global__ void __launch_bounds__(256) k_update_ur(int n, double* __restrict__ u64, T* __restrict__ uT, T* __restrict__ r,
+__device__ __forceinline__ void load_chunk(const T* __restrict__ src, T (&v)[Chunk<T>::CH]) {
+  using V = typename Chunk<T>::V;
+  const V* s = reinterpret_cast<const V*>(src);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) reinterpret_cast<V*>(v)[i] = s[i];
+}
+template <typename T>
+__device__ __forceinline__ void store_chunk(T* __restrict__ dst, const T (&v)[Chunk<T>::CH]) {
+  using V = typename Chunk<T>::V;
+  V* d = reinterpret_cast<V*>(dst);
+#pragma unroll
+  for (int i = 0; i < 3; ++i) d[i] = reinterpret_cast<const V*>(v)[i];
+}
+
+template <typename T, typename U>
+__global__ void __launch_bounds__(256) k_update_ur(int n, U* __restrict__ u, T* __restrict__ r,
                                                    const T* __restrict__ p, const T* __restrict__ q, LoadScalars* scal,
                                                    double* partials, int cap) {
+  constexpr int CH = Chunk<T>::CH;
   const size_t N = size_t(n) * n * n, N3 = 3 * N;
   const int load = blockIdx.y;
   LoadScalars& S = scal[load];
@@ -22,20 +44,31 @@ __global__ void __launch_bounds__(256) k_update_ur(int n, double* __restrict__ u
   const T a = T(alpha);
   const size_t off = size_t(load) * N3;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  // grid-stride over nodes: 3 components per node so the component sums stay per-thread
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+  const size_t nch = N3 / CH;
+  for (size_t ch = size_t(blockIdx.x) * blockDim.x + threadIdx.x; ch < nch; ch += size_t(gridDim.x) * blockDim.x) {
+    const size_t k = off + ch * CH;
+    T pv[CH], qv[CH], rv[CH];
+    load_chunk<T>(p + k, pv);
+    load_chunk<T>(q + k, qv);
+    load_chunk<T>(r + k, rv);
+    if constexpr (sizeof(U) == sizeof(T)) {
+      U uv[CH];
+      load_chunk<U>(u + k, uv);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const size_t k = off + 3 * i + c;
-      const T pv = p[k];
-      if (u64) u64[k] += alpha * double(pv);
-      else uT[k] += a * pv;
-      const T rv = r[k] - a * q[k];
-      r[k] = rv;
-      const double rd = double(rv);
-      acc[0] += rd * rd;
-      acc[1 + c] += rd;
+      for (int j = 0; j < CH; ++j) uv[j] += U(alpha) * U(pv[j]);
+      store_chunk<U>(u + k, uv);
+    } else {
+#pragma unroll
+      for (int j = 0; j < CH; ++j) u[k + j] += alpha * double(pv[j]);
     }
+#pragma unroll
+    for (int j = 0; j < CH; ++j) {
+      rv[j] = rv[j] - a * qv[j];
+      const double rd = double(rv[j]);
+      acc[0] += rd * rd;
+      acc[1 + j % 3] += rd;
+    }
+    store_chunk<T>(r + k, rv);
   }
   __shared__ double red[128];
   block_sum<4>(acc, red);
@@ -63,14 +96,20 @@ __global__ void __launch_bounds__(256) k_update_ur(int n, double* __restrict__ u
 
 int launch_update_ur(pgj_ctx* c, int loads, int prec, double* u64, void* uT, cudaStream_t s) {
   dim3 grid(2 * 148, loads);
-  if (prec == PGJ_FP32)
-    k_update_ur<float><<<grid, 256, 0, s>>>(c->n, u64, static_cast<float*>(uT), static_cast<float*>(c->r),
-                                            static_cast<const float*>(c->p), static_cast<const float*>(c->q), c->scal,
-                                            c->partials, 4000);
-  else
-    k_update_ur<double><<<grid, 256, 0, s>>>(c->n, u64, static_cast<double*>(uT), static_cast<double*>(c->r),
-                                             static_cast<const double*>(c->p), static_cast<const double*>(c->q),
-                                             c->scal, c->partials, 4000);
+  if (prec == PGJ_FP32) {
+    if (u64)
+      k_update_ur<float, double><<<grid, 256, 0, s>>>(c->n, u64, static_cast<float*>(c->r),
+                                                      static_cast<const float*>(c->p), static_cast<const float*>(c->q),
+                                                      c->scal, c->partials, 4000);
+    else
+      k_update_ur<float, float><<<grid, 256, 0, s>>>(c->n, static_cast<float*>(uT), static_cast<float*>(c->r),
+                                                     static_cast<const float*>(c->p), static_cast<const float*>(c->q),
+                                                     c->scal, c->partials, 4000);
+  } else {
+    k_update_ur<double, double><<<grid, 256, 0, s>>>(c->n, u64 ? u64 : static_cast<double*>(uT),
+                                                     static_cast<double*>(c->r), static_cast<const double*>(c->p),
+                                                     static_cast<const double*>(c->q), c->scal, c->partials, 4000);
+  }
   return check_launch();
 }
 
@@ -93,19 +132,24 @@ __global__ void __launch_bounds__(256) k_update_p(int n, int loads, T* __restric
   }
   const LoadScalars& S = scal[load];
   if (!S.active) return;
-  const T m0 = T(S.mean_z[0]), m1 = T(S.mean_z[1]), m2 = T(S.mean_z[2]);
+  constexpr int CH = Chunk<T>::CH;
+  const T m[3] = {T(S.mean_z[0]), T(S.mean_z[1]), T(S.mean_z[2])};
   const T beta = T(S.beta);
   const size_t off = size_t(load) * N3;
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3 / 3; i += size_t(gridDim.x) * blockDim.x) {
-    const size_t k = off + 3 * i;
-    const T z0 = sw[k] - m0, z1 = sw[k + 1] - m1, z2 = sw[k + 2] - m2;
+  const size_t nch = N3 / CH;
+  for (size_t ch = size_t(blockIdx.x) * blockDim.x + threadIdx.x; ch < nch; ch += size_t(gridDim.x) * blockDim.x) {
+    const size_t k = off + ch * CH;
+    T zv[CH], pv[CH];
+    load_chunk<T>(sw + k, zv);
     if (init) {
-      p[k] = z0; p[k + 1] = z1; p[k + 2] = z2;
+#pragma unroll
+      for (int j = 0; j < CH; ++j) pv[j] = zv[j] - m[j % 3];
     } else {
-      p[k] = z0 + beta * p[k];
-      p[k + 1] = z1 + beta * p[k + 1];
-      p[k + 2] = z2 + beta * p[k + 2];
+      load_chunk<T>(p + k, pv);
+#pragma unroll
+      for (int j = 0; j < CH; ++j) pv[j] = (zv[j] - m[j % 3]) + beta * pv[j];
     }
+    store_chunk<T>(p + k, pv);
   }
 }
 
@@ -134,6 +178,91 @@ __global__ void k_init_mask(int loads, LoadScalars* scal, int cap, int* body_run
 
 int launch_init_mask(pgj_ctx* c, int loads, cudaStream_t s) {
   k_init_mask<<<1, 32, 0, s>>>(loads, c->scal, 4000, c->cond);
+  return check_launch();
+}
+
+// ------------------------------------------------------------------------------ mixed refinement
+// Start of one refinement sweep, per load: the FP64 certificate decides whether the load still needs
+// a correction; r_in = T(r64), d = 0; the inner target is inner_rtol * ||r64||.
+template <typename T>
+__global__ void __launch_bounds__(256) k_inner_start(int n, const double* __restrict__ r64, T* __restrict__ r,
+                                                     T* __restrict__ d, const LoadScalars* out_scal,
+                                                     LoadScalars* in_scal, double* partials, double inner_rtol,
+                                                     int* body_runs) {
+  const size_t N = size_t(n) * n * n, N3 = 3 * N;
+  const int load = blockIdx.y;
+  const LoadScalars& O = out_scal[load];
+  LoadScalars& S = in_scal[load];
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) { body_runs[0] = 0; body_runs[1] = 0; }
+  const bool done = isfinite(O.absolute) && O.absolute * O.absolute <= O.target2 && !O.bad;
+  if (done) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) { S.active = 0; S.touched = 0; S.iterations = 0; }
+    return;
+  }
+  const size_t off = size_t(load) * N3;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const size_t k = off + 3 * i + c;
+      const T v = T(r64[k]);
+      r[k] = v;
+      d[k] = T(0);
+      const double dv = double(v);
+      acc[0] += dv * dv;
+      acc[1 + c] += dv;
+    }
+  }
+  __shared__ double red[128];
+  block_sum<4>(acc, red);
+  double* part = partials + size_t(load) * kPartialQ * kMaxPartials;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < 4; ++k) part[k * kMaxPartials + blockIdx.x] = acc[k];
+  if (!last_block(&S.ticket[kTicketUpdate], gridDim.x)) return;
+  if (threadIdx.x < 32) {
+    double v[4];
+    for (int k = 0; k < 4; ++k) v[k] = warp_sum_partials(part + k * kMaxPartials, gridDim.x);
+    if (threadIdx.x == 0) {
+      const double t = inner_rtol * O.absolute;
+      S.target2 = t * t;
+      S.res2 = v[0];
+      for (int c = 0; c < 3; ++c) S.mean_r[c] = v[1 + c] / double(N);
+      S.iterations = 0;
+      S.bad = 0;
+      S.failed = 0;
+      S.touched = 1;
+      S.active = (v[0] > S.target2) && isfinite(v[0]) ? 1 : 0;
+    }
+  }
+}
+
+// End of a sweep: x += d for touched loads; iteration and latch bookkeeping on the outer record.
+template <typename T>
+__global__ void __launch_bounds__(256) k_inner_finish(int n, double* __restrict__ x, const T* __restrict__ d,
+                                                      LoadScalars* out_scal, const LoadScalars* in_scal) {
+  const size_t N3 = 3 * size_t(n) * n * n;
+  const int load = blockIdx.y;
+  const LoadScalars& S = in_scal[load];
+  if (!S.touched) return;
+  const size_t off = size_t(load) * N3;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x)
+    x[off + i] += double(d[off + i]);
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    out_scal[load].total_iterations += S.iterations;
+    out_scal[load].bad |= S.bad;
+  }
+}
+
+int launch_inner_start(pgj_ctx* c, int loads, double inner_rtol, cudaStream_t s) {
+  dim3 grid(2 * 148, loads);
+  k_inner_start<float><<<grid, 256, 0, s>>>(c->n, c->r64, static_cast<float*>(c->r), static_cast<float*>(c->d),
+                                            c->scal_out, c->scal_in, c->partials, inner_rtol, c->cond);
+  return check_launch();
+}
+
+int launch_inner_finish(pgj_ctx* c, int loads, cudaStream_t s) {
+  dim3 grid(2 * 148, loads);
+  k_inner_finish<float><<<grid, 256, 0, s>>>(c->n, c->x, static_cast<const float*>(c->d), c->scal_out, c->scal_in);
   return check_launch();
 }
 

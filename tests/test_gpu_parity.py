@@ -260,3 +260,54 @@ def test_dense_fe_reference(pkg, golden_dir):
     assert rel(e, d["dense_energies"]) < 1e-9
     moduli = (e * a.reshape(1, -1)).mean(1)
     assert rel(moduli, d["dense_moduli"]) < 1e-9
+
+
+@pytest.mark.parametrize("n,emin", [(16, 1e-6), (24, 1e-9), (32, 1e-4)])
+def test_mixed_refinement_certifies_and_matches_fp64(pkg, oracle, n, emin):
+    """FP32 inner PCG inside FP64 refinement: FP64 certificate, C_H within 1e-7 of the FP64 oracle."""
+    lam, mu = pkg.PAPER_MEDIUM
+    a = pkg.baseline_design(n, seed=13, emin=emin)
+    ref = oracle.homogenize(a, lam, mu, 0.5) if n <= 24 else None
+    out = {}
+    for prec in ("fp64", "mixed"):
+        op = pkg.Operator(n, 6, lam, mu, precision=prec)
+        op.set_material(dev(a))
+        op.set_alpha(0.5)
+        u = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")
+        infos, st = op.solve(np.eye(6), 1e-8, u)
+        assert st == 0, (prec, infos)
+        assert all(i["converged"] and i["relative_residual"] <= 1e-8 for i in infos)
+        out[prec] = (op.effective_tensor(u).cpu().numpy(), op.last_refinements())
+    C64, Cmx = out["fp64"][0], out["mixed"][0]
+    assert rel(Cmx, C64) < 1e-7, rel(Cmx, C64)
+    if ref is not None:
+        assert rel(Cmx, ref["C"]) < 1e-7
+        assert rel(C64, ref["C"]) < 1e-10
+    assert 1 <= out["mixed"][1] <= 12
+
+
+def test_mixed_inner_tolerance_changes_sweeps(pkg):
+    n = 16
+    lam, mu = pkg.PAPER_MEDIUM
+    a = pkg.baseline_design(n, seed=2, emin=1e-6)
+    sweeps = []
+    for rtol_in in (1e-3, 1e-5):
+        op = pkg.Operator(n, 6, lam, mu, precision="mixed")
+        op.set_inner_rtol(rtol_in)
+        op.set_material(dev(a))
+        op.set_alpha(0.5)
+        u = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")
+        infos, st = op.solve(np.eye(6), 1e-8, u)
+        assert st == 0
+        sweeps.append(op.last_refinements())
+    assert sweeps[0] >= sweeps[1]
+
+
+def test_profile_iteration_reports_all_kernels(pkg):
+    n = 16
+    for prec in ("fp64", "mixed"):
+        op = pkg.Operator(n, 6, *pkg.PAPER_MEDIUM, precision=prec)
+        op.set_material(dev(pkg.baseline_design(n, seed=1, emin=1e-6)))
+        op.set_alpha(0.5)
+        prof = op.profile_iteration(np.eye(6), reps=3)
+        assert len(prof) == 8 and all(v["ms"] > 0 and v["bytes"] > 0 for v in prof.values())
