@@ -115,9 +115,18 @@ int pgj_green_symbol(int n, double lam, double mu, double* symbol, void* stream)
  * certificate and the stopping rule are the FP64 ones. */
 int pgj_solve(pgj_ctx* ctx, int loads, const double* macros, double rtol, double* u,
               pgj_load_info* info, void* stream);
-/* Inner relative tolerance of the FP32 refinement solve (default 1e-5). */
+/* Inner relative tolerance of the FP32 refinement sweeps (mode 1; default 1e-5). */
 int pgj_set_inner_rtol(pgj_ctx* ctx, double inner_rtol);
-/* Number of refinement sweeps taken by the last pgj_solve (1 for PGJ_FP64). */
+/* Mixed-precision scheme of a PGJ_FP32 context (no reference counterpart: the reference is FP64 only).
+ * mode 0 (default): one FP32 PCG recurrence per load with reliable updates; whenever the recurrence
+ * residual falls below delta times its value at the last replacement (or the recurrence reports
+ * convergence), the FP32 correction is added to the FP64 solution and the recurrence residual is
+ * replaced by the FP64 true residual f - K u, on the device, without restarting the Krylov space
+ * (delta in (0,1), default 0.1). mode 1: restarted refinement sweeps (FP32 solve to inner_rtol,
+ * u += d, FP64 residual), at most 12 sweeps. */
+int pgj_set_mixed_mode(pgj_ctx* ctx, int mode, double delta);
+/* Refinement count of the last pgj_solve: 1 for PGJ_FP64; sweeps in mixed mode 1; 1 + true-residual
+ * replacements in mixed mode 0. */
 int pgj_last_refinements(pgj_ctx* ctx);
 
 /* Kernel launches issued by the last pgj_solve (graph nodes included), for launch accounting. */

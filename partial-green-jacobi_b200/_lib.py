@@ -60,6 +60,7 @@ SIGNATURES = {
     "pgj_green_symbol": (C.c_int, [C.c_int, f64, f64, vp, vp]),
     "pgj_solve": (C.c_int, [vp, C.c_int, vp, f64, vp, C.POINTER(LoadInfo), vp]),
     "pgj_set_inner_rtol": (C.c_int, [vp, f64]),
+    "pgj_set_mixed_mode": (C.c_int, [vp, C.c_int, f64]),
     "pgj_last_refinements": (C.c_int, [vp]),
     "pgj_last_launches": (C.c_longlong, [vp]),
     "pgj_profile_iteration": (C.c_int, [vp, C.c_int, vp, C.c_int, vp, vp, vp]),

@@ -58,6 +58,8 @@ struct LoadScalars {
   int failed;       // set by the apply finalizer when p.q or rz is invalid
   int iterations;   // PCG iterations taken
   int touched;      // mixed refinement: this load ran an inner solve in the current sweep
+  int reliable;     // mixed: replace the FP32 recurrence residual by the FP64 true residual now
+  double anchor;    // mixed: recurrence ||r||^2 at the last true-residual replacement
   int total_iterations;  // mixed refinement: inner iterations summed over sweeps
   int ticket[8];    // per-kernel block tickets for the last-block finalizers
 };

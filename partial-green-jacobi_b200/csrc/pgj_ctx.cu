@@ -93,6 +93,83 @@ static int capture_iteration(pgj_ctx* c, int L, cudaStream_t s, cudaGraphConditi
   return launch_update_p(c, L, prec, false, s, h, last);
 }
 
+// Appends a conditional node of `type` after the current capture point of `s` and returns its body
+// graph; the capture of `s` continues after the node.
+static int add_conditional(cudaStream_t s, cudaGraphConditionalHandle* h, unsigned def, cudaGraphConditionalNodeType type,
+                           cudaGraph_t* body) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, &deps, &ndeps);
+  if (e == cudaSuccess && !*h) e = cudaGraphConditionalHandleCreate(h, cg, def, cudaGraphCondAssignDefault);
+  cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+  cp.conditional.handle = *h;
+  cp.conditional.type = type;
+  cp.conditional.size = 1;
+  cudaGraphNode_t node = nullptr;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&node, cg, deps, ndeps, &cp);
+  if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  *body = cp.conditional.phGraph_out[0];
+  return PGJ_OK;
+}
+
+// Creates a conditional handle in the graph being captured on `s` (for kernels that set it).
+static int make_handle(cudaStream_t s, cudaGraphConditionalHandle* h, unsigned def) {
+  cudaStreamCaptureStatus cs;
+  cudaGraph_t cg = nullptr;
+  cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &cg, nullptr, nullptr);
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(h, cg, def, cudaGraphCondAssignDefault);
+  return e == cudaSuccess ? PGJ_OK : set_cuda_error(e);
+}
+
+// Captures `fn(stream)` into `body` on a private stream.
+template <typename F>
+static int capture_into(cudaGraph_t body, F&& fn) {
+  cudaStream_t s2;
+  cudaError_t e = cudaStreamCreateWithFlags(&s2, cudaStreamNonBlocking);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  int st;
+  e = cudaStreamBeginCaptureToGraph(s2, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) {
+    st = set_cuda_error(e);
+  } else {
+    st = fn(s2);
+    cudaGraph_t bg = body;
+    cudaError_t e2 = cudaStreamEndCapture(s2, &bg);
+    if (!st && e2 != cudaSuccess) st = set_cuda_error(e2);
+  }
+  cudaStreamDestroy(s2);
+  return st;
+}
+
+// Mixed reliable-update iteration (FP32 recurrence, inner records active):
+// operator, update, IF(any load flagged){x += d; r64 = f - K64 x; r = T(r64)}, Green, p update.
+static int capture_iteration_rel(pgj_ctx* c, int L, cudaStream_t s, cudaGraphConditionalHandle hw) {
+  int st;
+  if ((st = launch_stencil(c, kPCG, L, PGJ_FP32, c->p, c->q, nullptr, nullptr, s))) return st;
+  if ((st = launch_update_ur(c, L, PGJ_FP32, nullptr, c->d, s))) return st;
+  cudaGraphConditionalHandle hif = 0;
+  if ((st = make_handle(s, &hif, 0))) return st;
+  if ((st = launch_rel_cond(c, L, hif, s))) return st;
+  cudaGraph_t ifbody = nullptr;
+  if ((st = add_conditional(s, &hif, 0, cudaGraphCondTypeIf, &ifbody))) return st;
+  st = capture_into(ifbody, [&](cudaStream_t s3) {
+    int r = launch_rel_fold(c, L, false, s3);
+    if (r) return r;
+    LoadScalars* saved = c->scal;
+    c->scal = c->scal_out;
+    r = launch_stencil(c, kResidual, L, PGJ_FP64, c->x, c->r64, c->f, nullptr, s3, c->scal_in);
+    c->scal = saved;
+    if (r) return r;
+    return launch_rel_sync(c, L, s3);
+  });
+  if (st) return st;
+  if ((st = launch_green(c, L, PGJ_FP32, c->r, false, s))) return st;
+  return launch_update_p(c, L, PGJ_FP32, false, s, hw, true);
+}
+
 static int end_capture(cudaStream_t s, cudaGraph_t* g, int st) {
   cudaError_t e = cudaStreamEndCapture(s, g);
   if (st) { if (*g) cudaGraphDestroy(*g); *g = nullptr; return st; }
@@ -101,7 +178,7 @@ static int end_capture(cudaStream_t s, cudaGraph_t* g, int st) {
 }
 
 // Appends to the capture on `s`: directions init, then WHILE(any load active){iteration}.
-static int capture_pcg(pgj_ctx* c, int L, cudaStream_t s) {
+static int capture_pcg(pgj_ctx* c, int L, cudaStream_t s, bool reliable = false) {
   int st = launch_green(c, L, c->prec, c->r, true, s);
   if (!st) st = launch_update_p(c, L, c->prec, true, s, 0, false);
   if (st) return st;
@@ -128,7 +205,7 @@ static int capture_pcg(pgj_ctx* c, int L, cudaStream_t s) {
   if (e != cudaSuccess) {
     st = set_cuda_error(e);
   } else {
-    st = capture_iteration(c, L, s2, h, true);
+    st = reliable ? capture_iteration_rel(c, L, s2, h) : capture_iteration(c, L, s2, h, true);
     cudaGraph_t bg = body;
     cudaError_t e2 = cudaStreamEndCapture(s2, &bg);
     if (!st && e2 != cudaSuccess) st = set_cuda_error(e2);
@@ -156,7 +233,15 @@ static int build_graphs(pgj_ctx* c, int L) {
   // FP64 attempt: init masks -> PCG loop -> certify.
   // Mixed sweep: r_in = T(r64), d = 0 -> inner PCG loop (FP32) -> x += d -> FP64 certify.
   if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return set_cuda_error(e);
-  if (c->prec == PGJ_FP32) {
+  if (c->prec == PGJ_FP32 && c->mixed_mode == 0) {
+    st = launch_rel_start(c, L, s);
+    if (!st) {
+      c->scal = c->scal_in;
+      st = capture_pcg(c, L, s, true);
+      c->scal = c->scal_out;
+    }
+    if (!st) st = launch_rel_fold(c, L, true, s);
+  } else if (c->prec == PGJ_FP32) {
     st = launch_inner_start(c, L, c->inner_rtol, s);
     if (!st) {
       c->scal = c->scal_in;
@@ -257,6 +342,8 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
   c->aux = reinterpret_cast<double*>(b + y.aux);
   c->alpha = 0.0;
   c->inner_rtol = 1e-5;
+  c->rel_delta2 = precision == PGJ_FP32 ? 1e-2 : 0.0;
+  c->mixed_mode = 0;
   c->last_refinements = 0;
   c->graphs = new (std::nothrow) Graphs();
   int st = PGJ_OK;
@@ -276,6 +363,7 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
     if (e != cudaSuccess) st = set_cuda_error(e);
   }
   if (!st) st = launch_scale(c, 0.0, s);  // scale = 1 until an alpha is selected
+  if (!st) st = autotune_stencil(c, s);
   if (st) {
     delete c->graphs;
     delete c;
@@ -353,6 +441,14 @@ int pgj_set_inner_rtol(pgj_ctx* c, double inner_rtol) {
 
 int pgj_last_refinements(pgj_ctx* c) { return c ? c->last_refinements : -1; }
 
+int pgj_set_mixed_mode(pgj_ctx* c, int mode, double delta) {
+  if (!c || (mode != 0 && mode != 1) || !(delta > 0 && delta < 1)) return PGJ_ERR_ARGUMENT;
+  c->mixed_mode = mode;
+  c->rel_delta2 = c->prec == PGJ_FP32 ? delta * delta : 0.0;
+  c->graphs->loads = 0;  // rebuild the solve graphs with the new scheme
+  return PGJ_OK;
+}
+
 // Maximum FP64 refinement sweeps of the mixed solve (each sweep: one FP32 inner PCG solve to
 // inner_rtol relative, x += d, FP64 certification).
 static constexpr int kMaxSweeps = 12;
@@ -361,7 +457,7 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
   if (!c || !macros || !u || !info || loads < 1 || loads > c->L || !(rtol > 0)) return PGJ_ERR_ARGUMENT;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const size_t N3 = 3 * size_t(c->N);
-  const bool mixed = c->prec == PGJ_FP32;
+  const bool mixed = c->prec == PGJ_FP32 && c->mixed_mode == 1;  // restarted refinement sweeps
   c->scal = c->scal_out;
   int st = stage_macros(c, loads, macros, s);
   if (!st) st = launch_rhs(c, loads, c->macros, c->f, s);
@@ -371,11 +467,12 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
   if (u != c->x) e = cudaMemcpyAsync(c->x, u, sizeof(double) * N3 * loads, cudaMemcpyDeviceToDevice, s);
   if (e != cudaSuccess) return set_cuda_error(e);
   if ((st = build_graphs(c, loads))) return st;
+  if ((e = cudaMemsetAsync(c->cond + 2, 0, sizeof(int), s)) != cudaSuccess) return set_cuda_error(e);
   if ((e = cudaGraphLaunch(c->graphs->cert, s)) != cudaSuccess) return set_cuda_error(e);
   std::vector<LoadScalars> h(loads);
   std::vector<int> ok(loads, 0);
   int restarts = 0, sweeps = 0;
-  int body[2] = {0, 0};
+  int body[4] = {0, 0, 0, 0};
   long long launches = 2 + 3;  // rhs + norms, initial certification
   bool capped_by_bound = false;
   auto read_state = [&](bool with_body) -> cudaError_t {
@@ -413,8 +510,10 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
     for (;;) {
       if ((e = cudaGraphLaunch(c->graphs->attempt, s)) != cudaSuccess) return set_cuda_error(e);
       if ((e = read_state(true)) != cudaSuccess) return set_cuda_error(e);
-      // attempt: init mask + 5 Green passes + p init, 8 kernels per loop body, 3 certification kernels
-      launches += 7 + 8LL * body[0] + 3;
+      if (c->prec == PGJ_FP32)  // rel start + Green + p init, 9 per body, 3 per replacement, fold + certify
+        launches += 7 + 9LL * body[0] + 3LL * body[3] + 1 + 3;
+      else  // attempt: init mask + 5 Green passes + p init, 8 kernels per loop body, 3 certification kernels
+        launches += 7 + 8LL * body[0] + 3;
       if (body[1]) { capped_by_bound = true; break; }
       bool all, anybad, capped;
       evaluate(all, anybad, capped);
@@ -440,8 +539,9 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
     I.bad = h[l].bad;
     all = all && ok[l];
   }
-  c->last_refinements = mixed ? sweeps : 1;
+  c->last_refinements = mixed ? sweeps : (c->prec == PGJ_FP32 ? 1 + body[3] : 1);
   c->last_launches = launches;
+  if (body[2]) return PGJ_ERR_TIMEOUT;
   if (capped_by_bound) return PGJ_ERR_ITERATION_CAP;
   return all ? PGJ_OK : PGJ_ERR_CERTIFICATION;
 }

@@ -65,7 +65,7 @@ FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan) {
   };
   g.thr_x = threads(3 * g.rb / 2);
   g.thr_y = threads(g.kcy);
-  g.thr_z = threads(3 * g.kcz);
+  g.thr_z = threads(3 * g.kcz) > 256 ? 256 : threads(3 * g.kcz);
   return g;
 }
 

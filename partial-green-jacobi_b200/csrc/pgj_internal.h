@@ -23,6 +23,7 @@ struct StencilGeom {
   int threads() const { return 0; }
 };
 StencilGeom stencil_geom(int n, int loads);
+StencilGeom stencil_geom_shape(int n, int ty, int zc);
 
 // Geometry of the FFT passes.
 struct FFTGeom {
@@ -44,10 +45,13 @@ struct StencilArgs {
   void* out;
   const double* f;             // residual mode: right-hand side
   const int32_t* active_ext;   // plain mode: optional external mask
+  const LoadScalars* rel_flags; // residual mode: when set, only loads with rel_flags[l].reliable
   LoadScalars* scal;           // pcg / residual modes
   double* partials;            // [load][4][nblk]
   OpConst kc;
   int iteration_cap;
+  int tma;                     // stage planes with bulk async copies (aligned rows) instead of cp.async
+  int* err;                    // set to 1 if a bounded device wait expired
 };
 
 // Partial-sum slots per load per kernel (blocks per load upper bound).
@@ -106,6 +110,8 @@ struct pgj_ctx {
   double* aux;         // (64 + kMaxPartials) doubles: small staged tables and scalar reductions
   double alpha;
   double inner_rtol;
+  double rel_delta2;   // mixed reliable updates: replace r when ||r||^2 < rel_delta2 * anchor (0 = off)
+  int mixed_mode;      // 0 reliable-update CG, 1 restarted refinement sweeps
   int last_refinements;
   long long last_launches;
   pgj::Graphs* graphs;
@@ -114,7 +120,7 @@ struct pgj_ctx {
 namespace pgj {
 // operator (pgj_operator.cu)
 int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, void* out, const double* f,
-                   const int32_t* active_ext, cudaStream_t s);
+                   const int32_t* active_ext, cudaStream_t s, const LoadScalars* rel_flags = nullptr);
 int launch_rhs(pgj_ctx* c, int loads, const double* macros_dev, double* f, cudaStream_t s);
 int launch_scale(pgj_ctx* c, double alpha, cudaStream_t s);
 int launch_project_u(pgj_ctx* c, int loads, double* u, cudaStream_t s);
@@ -137,6 +143,11 @@ int launch_init_mask(pgj_ctx* c, int loads, cudaStream_t s);
 // then x += d for the loads solved in this sweep
 int launch_inner_start(pgj_ctx* c, int loads, double inner_rtol, cudaStream_t s);
 int launch_inner_finish(pgj_ctx* c, int loads, cudaStream_t s);
+// reliable-update mixed solve (pgj_pcg.cu)
+int launch_rel_start(pgj_ctx* c, int loads, cudaStream_t s);
+int launch_rel_cond(pgj_ctx* c, int loads, cudaGraphConditionalHandle h, cudaStream_t s);
+int launch_rel_fold(pgj_ctx* c, int loads, bool all, cudaStream_t s);
+int launch_rel_sync(pgj_ctx* c, int loads, cudaStream_t s);
 // energy (pgj_energy.cu)
 int launch_energies(pgj_ctx* c, int loads, const double* u, const double* macros_dev, double* e, cudaStream_t s);
 int launch_effective_tensor(pgj_ctx* c, const double* u, double* C, double* e, cudaStream_t s);
@@ -144,6 +155,8 @@ int launch_effective_tensor(pgj_ctx* c, const double* u, double* C, double* e, c
 int set_cuda_error(cudaError_t e);
 // one-time kernel attributes (dynamic shared memory limits); called at context creation
 int prepare_stencil_kernels();
+// times candidate tile shapes of the operator on the context's buffers and keeps the fastest
+int autotune_stencil(pgj_ctx* c, cudaStream_t s);
 int prepare_fft_kernels();
 inline int check_launch() {
   cudaError_t e = cudaGetLastError();

@@ -13,6 +13,10 @@
 #include "pgj_internal.h"
 #include <cmath>
 #include <cstdlib>
+#include <map>
+#include <mutex>
+#include <tuple>
+#include <vector>
 
 namespace pgj {
 
@@ -29,6 +33,60 @@ template <> __device__ __forceinline__ void cp_async<float>(float* dst, const fl
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 __device__ __forceinline__ void cp_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// --- TMA (bulk async copy) staging: one elected thread copies whole rows into shared memory and
+// the block waits on an mbarrier whose transaction count is the plane's byte size.
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void tma_row(void* dst, const void* src, unsigned bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after kMaxTries polls (each poll may suspend briefly in hardware).
+constexpr int kMaxTries = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  for (int i = 0; i < kMaxTries; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+template <typename T>
+__device__ __forceinline__ void tma_plane(T* buf, const T* in, int pz, int y0, int rows, int n, uint64_t* bar) {
+  const unsigned rowbytes = unsigned(3 * n * sizeof(T));
+  fence_proxy_async();
+  mbar_expect_tx(bar, rowbytes * rows);
+  for (int r = 0; r < rows; ++r) {
+    int y = (y0 - 1 + r) % n;
+    if (y < 0) y += n;
+    tma_row(buf + r * 3 * n, in + (size_t(pz) * n + y) * size_t(3 * n), rowbytes, bar);
+  }
+}
+
+StencilGeom stencil_geom_shape(int n, int ty, int zc) {
+  StencilGeom g;
+  g.ty = ty;
+  g.ntiles = (n + ty - 1) / ty;
+  g.zc = zc;
+  g.nchunks = (n + zc - 1) / zc;
+  return g;
+}
 
 StencilGeom stencil_geom(int n, int loads) {
   StencilGeom g;
@@ -111,6 +169,7 @@ __global__ void __launch_bounds__(512, 1) k_stencil(const StencilArgs A) {
   bool act = true;
   if (MODE == kPCG) act = A.scal[load].active != 0;
   else if (A.active_ext) act = A.active_ext[load] != 0;
+  else if (MODE == kResidual && A.rel_flags) act = A.rel_flags[load].reliable != 0;
   T* out = reinterpret_cast<T*>(A.out) + size_t(load) * 3 * N;
   if (!act) {
     if (MODE == kPlain && out_row) {
@@ -130,12 +189,32 @@ __global__ void __launch_bounds__(512, 1) k_stencil(const StencilArgs A) {
   T* upx = upy + (TY + 1) * n * 6;         // (TY+1) * n * 3
   double* red = reinterpret_cast<double*>(upx + (TY + 1) * n * 3 + 2);  // 32 * 4, 16-byte padded
   red = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(red) + 15) & ~uintptr_t(15));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(red + 32 * 4);  // two mbarriers (TMA staging)
+  const bool tma = A.tma != 0;
 
-  // prologue: planes z0-1 and z0
-  stage_plane(buf0, in, (z0 - 1 + n) % n, y0, TY + 2, n, tid, nthr);
-  stage_plane(buf1, in, z0 % n, y0, TY + 2, n, tid, nthr);
-  cp_wait_one();
-  __syncthreads();
+  // prologue: planes z0-1 (j = 0, buffer 0) and z0 (j = 1, buffer 1)
+  if (tma) {
+    if (tid == 0) {
+      mbar_init(&bars[0], 1);
+      mbar_init(&bars[1], 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0) {
+      tma_plane(buf0, in, (z0 - 1 + n) % n, y0, TY + 2, n, &bars[0]);
+      tma_plane(buf1, in, z0 % n, y0, TY + 2, n, &bars[1]);
+    }
+    const bool okw = mbar_wait(&bars[0], 0);
+    if (__syncthreads_or(!okw)) {
+      if (tid == 0 && A.err) atomicExch(A.err, 1);
+      return;
+    }
+  } else {
+    stage_plane(buf0, in, (z0 - 1 + n) % n, y0, TY + 2, n, tid, nthr);
+    stage_plane(buf1, in, z0 % n, y0, TY + 2, n, tid, nthr);
+    cp_wait_one();
+    __syncthreads();
+  }
   T F0[4][3], own[3], dummy[3];
   face_modes(buf0, ty, tx, n, F0, dummy);
   T Up[4][3];
@@ -153,10 +232,20 @@ __global__ void __launch_bounds__(512, 1) k_stencil(const StencilArgs A) {
     const int ez = z0 - 1 + s;           // element plane
     const int ezw = (ez + n) % n;
     const T ae = T(__ldg(aa + (size_t(ezw) * n + eyw) * n + tx));
-    cp_wait_all();
-    __syncthreads();
     T* cur = ((s + 1) & 1) ? buf1 : buf0;
-    if (s < zc) stage_plane(((s & 1) ? buf1 : buf0), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
+    if (tma) {
+      // plane j = s + 1 sits in buffer (s+1)&1, use number (s+1)>>1
+      const bool okw = mbar_wait(&bars[(s + 1) & 1], ((s + 1) >> 1) & 1);
+      if (__syncthreads_or(!okw)) {
+        if (tid == 0 && A.err) atomicExch(A.err, 1);
+        return;
+      }
+      if (s < zc && tid == 0) tma_plane(((s & 1) ? buf1 : buf0), in, (z0 + s + 1) % n, y0, TY + 2, n, &bars[s & 1]);
+    } else {
+      cp_wait_all();
+      __syncthreads();
+      if (s < zc) stage_plane(((s & 1) ? buf1 : buf0), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
+    }
 
     T F1[4][3], own1[3];
     face_modes(cur, ty, tx, n, F1, own1);
@@ -270,6 +359,58 @@ __global__ void __launch_bounds__(512, 1) k_stencil(const StencilArgs A) {
   }
 }
 
+// Tile autotuner: times the operator (all loads, plain mode) for candidate tile shapes on the
+// context's own buffers and keeps the fastest. Results are cached per (n, loads, precision) for the
+// process, so contexts created later reuse the choice.
+static std::mutex g_tune_mutex;
+static std::map<std::tuple<int, int, int>, StencilGeom> g_tuned;
+
+int autotune_stencil(pgj_ctx* c, cudaStream_t s) {
+  const int n = c->n;
+  const auto key = std::make_tuple(n, c->L, c->prec);
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) { c->sg = it->second; return PGJ_OK; }
+  }
+  if (std::getenv("PGJ_STENCIL_TY") || std::getenv("PGJ_STENCIL_ZC")) return PGJ_OK;  // manual override
+  std::vector<int> tys;
+  for (int ty : {1, 2, 3, 4, 5, 6, 7, 8, 12, 16, 31})
+    if (ty <= n && n * (ty + 1) <= 512 && (ty + 1) * n >= 32) tys.push_back(ty);
+  if (tys.empty()) tys.push_back(c->sg.ty);
+  std::vector<int> zcs;
+  for (int zc : {4, 8, 16, 32})
+    if (zc <= n) zcs.push_back(zc);
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  StencilGeom best = c->sg;
+  float best_ms = 1e30f;
+  const void* in = c->p;
+  void* out = c->q;
+  for (int ty : tys)
+    for (int zc : zcs) {
+      StencilGeom g = stencil_geom_shape(n, ty, zc);
+      if (g.ntiles * g.nchunks > kMaxPartials) continue;
+      c->sg = g;
+      int st = launch_stencil(c, kPlain, c->L, c->prec, in, out, nullptr, nullptr, s);  // warm
+      if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
+      cudaEventRecord(e0, s);
+      for (int r = 0; r < 3; ++r) launch_stencil(c, kPlain, c->L, c->prec, in, out, nullptr, nullptr, s);
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) { best_ms = ms; best = g; }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->sg = best;
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  g_tuned[key] = best;
+  return check_launch();
+}
+
 int prepare_stencil_kernels() {
   const int lim = 220 * 1024;  // below the 227 KB opt-in less the static shared memory
   cudaFuncSetAttribute(k_stencil<float, kPlain>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
@@ -281,15 +422,19 @@ int prepare_stencil_kernels() {
 }
 
 int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, void* out, const double* f,
-                   const int32_t* active_ext, cudaStream_t s) {
+                   const int32_t* active_ext, cudaStream_t s, const LoadScalars* rel_flags) {
   const int n = c->n;
   StencilArgs A;
   A.n = n; A.ty = c->sg.ty; A.zc = c->sg.zc;
   A.a = c->a; A.in = in; A.out = out; A.f = f; A.active_ext = active_ext;
   A.scal = c->scal; A.partials = c->partials; A.kc = c->kc; A.iteration_cap = 4000;
-  dim3 grid(c->sg.ntiles, c->sg.nchunks, loads), block(n, c->sg.ty + 1);
+  A.err = c->cond + 2;
+  A.rel_flags = rel_flags;
   const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
-  const size_t smem = tsz * (size_t(2) * (c->sg.ty + 2) * 3 * n + size_t(c->sg.ty + 1) * n * 9) + 32 * 4 * 8 + 64;
+  // TMA rows need 16-byte aligned starts and sizes: (3 n * element size) % 16 == 0 and an aligned base
+  A.tma = ((3 * size_t(n) * tsz) % 16 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0) ? 1 : 0;
+  dim3 grid(c->sg.ntiles, c->sg.nchunks, loads), block(n, c->sg.ty + 1);
+  const size_t smem = tsz * (size_t(2) * (c->sg.ty + 2) * 3 * n + size_t(c->sg.ty + 1) * n * 9) + 32 * 4 * 8 + 16 + 64;
   if (c->sg.ntiles * c->sg.nchunks > kMaxPartials) return PGJ_ERR_UNSUPPORTED;
   if (prec == PGJ_FP32) {
     switch (mode) {

@@ -34,7 +34,7 @@ __device__ __forceinline__ void store_chunk(T* __restrict__ dst, const T (&v)[Ch
 template <typename T, typename U>
 __global__ void __launch_bounds__(256) k_update_ur(int n, U* __restrict__ u, T* __restrict__ r,
                                                    const T* __restrict__ p, const T* __restrict__ q, LoadScalars* scal,
-                                                   double* partials, int cap) {
+                                                   double* partials, int cap, double rel_delta2) {
   constexpr int CH = Chunk<T>::CH;
   const size_t N = size_t(n) * n * n, N3 = 3 * N;
   const int load = blockIdx.y;
@@ -90,25 +90,32 @@ __global__ void __launch_bounds__(256) k_update_ur(int n, U* __restrict__ u, T* 
       S.active = keep ? 1 : 0;
       S.res2 = res2;
       for (int c = 0; c < 3; ++c) S.mean_r[c] = v[1 + c] / double(N);
+      if (rel_delta2 > 0.0) {
+        // reliable update: the recurrence residual fell by 1/delta since the last replacement, or the
+        // recurrence believes it has converged; the FP64 true residual decides.
+        const bool ok = valid && finite && it < cap;
+        S.reliable = ok && ((keep && res2 < rel_delta2 * S.anchor) || (!keep && res2 <= S.target2)) ? 1 : 0;
+      }
     }
   }
 }
 
 int launch_update_ur(pgj_ctx* c, int loads, int prec, double* u64, void* uT, cudaStream_t s) {
   dim3 grid(2 * 148, loads);
+  const double rel = c->rel_delta2;
   if (prec == PGJ_FP32) {
     if (u64)
       k_update_ur<float, double><<<grid, 256, 0, s>>>(c->n, u64, static_cast<float*>(c->r),
                                                       static_cast<const float*>(c->p), static_cast<const float*>(c->q),
-                                                      c->scal, c->partials, 4000);
+                                                      c->scal, c->partials, 4000, rel);
     else
       k_update_ur<float, float><<<grid, 256, 0, s>>>(c->n, static_cast<float*>(uT), static_cast<float*>(c->r),
                                                      static_cast<const float*>(c->p), static_cast<const float*>(c->q),
-                                                     c->scal, c->partials, 4000);
+                                                     c->scal, c->partials, 4000, rel);
   } else {
     k_update_ur<double, double><<<grid, 256, 0, s>>>(c->n, u64 ? u64 : static_cast<double*>(uT),
                                                      static_cast<double*>(c->r), static_cast<const double*>(c->p),
-                                                     static_cast<const double*>(c->q), c->scal, c->partials, 4000);
+                                                     static_cast<const double*>(c->q), c->scal, c->partials, 4000, rel);
   }
   return check_launch();
 }
@@ -263,6 +270,110 @@ int launch_inner_start(pgj_ctx* c, int loads, double inner_rtol, cudaStream_t s)
 int launch_inner_finish(pgj_ctx* c, int loads, cudaStream_t s) {
   dim3 grid(2 * 148, loads);
   k_inner_finish<float><<<grid, 256, 0, s>>>(c->n, c->x, static_cast<const float*>(c->d), c->scal_out, c->scal_in);
+  return check_launch();
+}
+
+// ------------------------------------------------------------------------------ reliable updates
+// Mixed solve: one FP32 CG recurrence per load; at chosen iterations the FP32 correction d is folded
+// into the FP64 solution x and the recurrence residual is replaced by the FP64 true residual f - K x.
+
+// r_in = T(r64), d = 0, recurrence scalars from the FP64 certificate (attempt start)
+template <typename T>
+__global__ void __launch_bounds__(256) k_rel_start(int n, const double* __restrict__ r64, T* __restrict__ r,
+                                                   T* __restrict__ d, const LoadScalars* out, LoadScalars* in, int cap,
+                                                   int* body_runs) {
+  const size_t N3 = 3 * size_t(n) * n * n;
+  const int load = blockIdx.y;
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) { body_runs[0] = 0; body_runs[1] = 0; body_runs[3] = 0; }
+  const size_t off = size_t(load) * N3;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x) {
+    r[off + i] = T(r64[off + i]);
+    d[off + i] = T(0);
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    const LoadScalars& O = out[load];
+    LoadScalars& S = in[load];
+    S.res2 = O.res2;
+    S.anchor = O.res2;
+    S.target2 = O.target2;
+    for (int c = 0; c < 3; ++c) S.mean_r[c] = O.mean_r[c];
+    S.iterations = O.iterations;
+    S.bad = O.bad;
+    S.failed = 0;
+    S.reliable = 0;
+    S.active = (O.res2 > O.target2) && (O.iterations < cap) && !O.bad ? 1 : 0;
+  }
+}
+
+// IF-node condition: any load flagged for a true-residual replacement
+__global__ void k_rel_cond(int loads, const LoadScalars* in, cudaGraphConditionalHandle h, int* counters) {
+  if (threadIdx.x != 0) return;
+  int any = 0;
+  for (int l = 0; l < loads; ++l) any |= in[l].reliable;
+  if (any) counters[3] += 1;  // replacements taken (launch accounting)
+  cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
+// x += d, d = 0 for flagged loads (all loads when `all`)
+template <typename T>
+__global__ void __launch_bounds__(256) k_rel_fold(int n, double* __restrict__ x, T* __restrict__ d,
+                                                  const LoadScalars* in, LoadScalars* out, int all) {
+  const size_t N3 = 3 * size_t(n) * n * n;
+  const int load = blockIdx.y;
+  if (!all && !in[load].reliable) return;
+  if (all && blockIdx.x == 0 && threadIdx.x == 0) {
+    // end of the attempt: the recurrence's bookkeeping becomes the certificate's
+    out[load].iterations = in[load].iterations;
+    out[load].bad |= in[load].bad;
+  }
+  const size_t off = size_t(load) * N3;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x) {
+    x[off + i] += double(d[off + i]);
+    d[off + i] = T(0);
+  }
+}
+
+// flagged loads: r_in = T(r64) (the true residual the FP64 operator just produced); the last block
+// resets the recurrence scalars to it and decides whether the load keeps iterating
+template <typename T>
+__global__ void __launch_bounds__(256) k_rel_sync(int n, const double* __restrict__ r64, T* __restrict__ r,
+                                                  const LoadScalars* out, LoadScalars* in, int cap) {
+  const size_t N3 = 3 * size_t(n) * n * n;
+  const int load = blockIdx.y;
+  LoadScalars& S = in[load];
+  if (!S.reliable) return;
+  const size_t off = size_t(load) * N3;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x)
+    r[off + i] = T(r64[off + i]);
+  if (!last_block(&S.ticket[kTicketAux2], gridDim.x)) return;
+  if (threadIdx.x == 0) {
+    const LoadScalars& O = out[load];
+    S.res2 = O.res2;
+    S.anchor = O.res2;
+    for (int c = 0; c < 3; ++c) S.mean_r[c] = O.mean_r[c];
+    S.active = isfinite(O.res2) && O.res2 > S.target2 && S.iterations < cap && !S.bad ? 1 : 0;
+    S.reliable = 0;
+  }
+}
+
+int launch_rel_start(pgj_ctx* c, int loads, cudaStream_t s) {
+  k_rel_start<float><<<dim3(2 * 148, loads), 256, 0, s>>>(c->n, c->r64, static_cast<float*>(c->r),
+                                                          static_cast<float*>(c->d), c->scal_out, c->scal_in, 4000,
+                                                          c->cond);
+  return check_launch();
+}
+int launch_rel_cond(pgj_ctx* c, int loads, cudaGraphConditionalHandle h, cudaStream_t s) {
+  k_rel_cond<<<1, 32, 0, s>>>(loads, c->scal_in, h, c->cond);
+  return check_launch();
+}
+int launch_rel_fold(pgj_ctx* c, int loads, bool all, cudaStream_t s) {
+  k_rel_fold<float><<<dim3(2 * 148, loads), 256, 0, s>>>(c->n, c->x, static_cast<float*>(c->d), c->scal_in,
+                                                         c->scal_out, all ? 1 : 0);
+  return check_launch();
+}
+int launch_rel_sync(pgj_ctx* c, int loads, cudaStream_t s) {
+  k_rel_sync<float><<<dim3(2 * 148, loads), 256, 0, s>>>(c->n, c->r64, static_cast<float*>(c->r), c->scal_out,
+                                                         c->scal_in, 4000);
   return check_launch();
 }
 

@@ -199,6 +199,12 @@ class Operator:
     def set_inner_rtol(self, rtol: float) -> None:
         _lib.check(_lib.lib().pgj_set_inner_rtol(self._ctx, float(rtol)), "pgj_set_inner_rtol")
 
+    def set_mixed_mode(self, mode: str = "reliable", delta: float = 0.1) -> None:
+        """``"reliable"``: one FP32 recurrence with FP64 true-residual replacements; ``"sweeps"``:
+        restarted refinement sweeps."""
+        m = {"reliable": 0, "sweeps": 1}[mode]
+        _lib.check(_lib.lib().pgj_set_mixed_mode(self._ctx, m, float(delta)), "pgj_set_mixed_mode")
+
     def last_refinements(self) -> int:
         return int(_lib.lib().pgj_last_refinements(self._ctx))
 

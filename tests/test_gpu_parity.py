@@ -263,7 +263,7 @@ def test_dense_fe_reference(pkg, golden_dir):
 
 
 @pytest.mark.parametrize("n,emin", [(16, 1e-6), (24, 1e-9), (32, 1e-4)])
-def test_mixed_refinement_certifies_and_matches_fp64(pkg, oracle, n, emin):
+def test_mixed_reliable_updates_certify_and_match_fp64(pkg, oracle, n, emin):
     """FP32 inner PCG inside FP64 refinement: FP64 certificate, C_H within 1e-7 of the FP64 oracle."""
     lam, mu = pkg.PAPER_MEDIUM
     a = pkg.baseline_design(n, seed=13, emin=emin)
@@ -277,13 +277,16 @@ def test_mixed_refinement_certifies_and_matches_fp64(pkg, oracle, n, emin):
         infos, st = op.solve(np.eye(6), 1e-8, u)
         assert st == 0, (prec, infos)
         assert all(i["converged"] and i["relative_residual"] <= 1e-8 for i in infos)
-        out[prec] = (op.effective_tensor(u).cpu().numpy(), op.last_refinements())
+        out[prec] = (op.effective_tensor(u).cpu().numpy(), op.last_refinements(),
+                     max(i["iterations"] for i in infos))
     C64, Cmx = out["fp64"][0], out["mixed"][0]
+    # one FP32 recurrence with true-residual replacements needs about the FP64 iteration count
+    assert out["mixed"][2] <= 1.5 * out["fp64"][2] + 20, (out["mixed"][2], out["fp64"][2])
     assert rel(Cmx, C64) < 1e-7, rel(Cmx, C64)
     if ref is not None:
         assert rel(Cmx, ref["C"]) < 1e-7
         assert rel(C64, ref["C"]) < 1e-10
-    assert 1 <= out["mixed"][1] <= 12
+    assert out["mixed"][1] >= 1
 
 
 def test_mixed_inner_tolerance_changes_sweeps(pkg):
@@ -293,6 +296,7 @@ def test_mixed_inner_tolerance_changes_sweeps(pkg):
     sweeps = []
     for rtol_in in (1e-3, 1e-5):
         op = pkg.Operator(n, 6, lam, mu, precision="mixed")
+        op.set_mixed_mode("sweeps")
         op.set_inner_rtol(rtol_in)
         op.set_material(dev(a))
         op.set_alpha(0.5)
