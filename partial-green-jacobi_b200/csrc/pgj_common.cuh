@@ -17,6 +17,28 @@ constexpr int kMaxStages = 8;
 
 __host__ __device__ __forceinline__ int wrapi(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
 
+// --------------------------------------------------------------------------- fast division
+// Quotient of a non-negative int below 2^31 by a fixed divisor d with one multiply-high and a
+// shift: m = ceil(2^p / d), p = 31 + ceil(log2 d) (the divisor-reciprocal method; checked
+// exhaustively on the host for the divisors used here).
+struct FastDiv {
+  unsigned d, m, s;
+};
+inline FastDiv make_fastdiv(unsigned d) {
+  FastDiv f;
+  f.d = d;
+  if (d <= 1) { f.m = 0; f.s = 0; return f; }
+  unsigned l = 0;
+  while ((1u << l) < d) ++l;
+  const unsigned p = 31 + l;
+  f.m = unsigned(((1ull << p) + d - 1) / d);
+  f.s = p - 32;
+  return f;
+}
+__device__ __forceinline__ int fdiv(int x, const FastDiv& f) {
+  return f.d <= 1 ? x : int(__umulhi(unsigned(x), f.m) >> f.s);
+}
+
 // --------------------------------------------------------------------------- complex
 template <typename T> struct Cx;
 template <> struct Cx<double> { using type = double2; };
@@ -66,12 +88,17 @@ struct LoadScalars {
 
 enum Ticket { kTicketApply = 0, kTicketUpdate = 1, kTicketFZ = 2, kTicketIFX = 3, kTicketAux = 4, kTicketAux2 = 5 };
 
+__device__ __forceinline__ int flat_tid() {
+  return threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+}
+__device__ __forceinline__ int block_threads() { return blockDim.x * blockDim.y * blockDim.z; }
+
 // Returns true in exactly one block per load: the last one to arrive. Every block that calls it
 // must have written its partials first. Resets the ticket for the next launch.
 __device__ __forceinline__ bool last_block(int* ticket, int nblocks) {
   __shared__ int amlast;
   __syncthreads();
-  if (threadIdx.x == 0 && threadIdx.y == 0) {
+  if (flat_tid() == 0) {
     __threadfence();
     int t = atomicAdd(ticket, 1);
     amlast = (t == nblocks - 1);
@@ -102,8 +129,8 @@ __device__ __forceinline__ double warp_reduce(double v, int lane, int active) {
 // (>= NV * 32 doubles).
 template <int NV>
 __device__ __forceinline__ void block_sum(double (&v)[NV], double* red) {
-  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-  const int nthreads = blockDim.x * blockDim.y;
+  const int tid = flat_tid();
+  const int nthreads = block_threads();
   const int warp = tid >> 5, lane = tid & 31, nwarps = (nthreads + 31) >> 5;
   const int active = min(32, nthreads - (warp << 5));
 #pragma unroll
@@ -125,8 +152,8 @@ __device__ __forceinline__ void block_sum(double (&v)[NV], double* red) {
 // Fixed-order sum of `count` partials by the first warp of the block (which may be partial);
 // call from every thread with tid < 32; result in thread 0.
 __device__ __forceinline__ double warp_sum_partials(const double* p, int count) {
-  const int tid = threadIdx.x + blockDim.x * threadIdx.y;
-  const int active = min(32, int(blockDim.x * blockDim.y));
+  const int tid = flat_tid();
+  const int active = min(32, block_threads());
   double s = 0.0;
   for (int i = tid; i < count; i += active) s += __ldcg(p + i);
   return warp_reduce(s, tid, active);

@@ -28,6 +28,11 @@ bool make_fft_plan(int n, FFTPlan* plan) {
   while (m % 2 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 2; m /= 2; }
   while (m % 3 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 3; m /= 3; }
   while (m % 5 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 5; m /= 5; }
+  int ns = 1;
+  for (int i = 0; i < plan->nst; ++i) {
+    plan->ns_div[i] = make_fastdiv(unsigned(ns));
+    ns *= plan->radix[i];
+  }
   return m == 1 && n % 2 == 0 && n >= 4;
 }
 
@@ -39,33 +44,41 @@ FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan) {
   const size_t cb = 2 * size_t(elem_bytes);  // complex bytes
   const size_t line = size_t(n + 1) * cb;
   const int ns = n / 2 + 1;
-  // x passes: rb rows -> 3 rb / 2 complex lines; keep <= ~48 lines and rb | n*n
-  int rb = 16;
-  while (rb > 2 && ((size_t(n) * n) % rb != 0 || 2 * (3 * size_t(rb) / 2) * line > kFFTSmemBudget)) rb /= 2;
-  g.rb = rb;
-  // y passes: kcy kx columns per block
-  int kcy = ns;
-  while (kcy > 1 && 2 * size_t(kcy) * line > kFFTSmemBudget) kcy = (kcy + 1) / 2;
-  g.kcy = kcy;
-  g.nky = (ns + kcy - 1) / kcy;
-  int kcz = ns;
-  while (kcz > 1 && 2 * 3 * size_t(kcz) * line > kFFTSmemBudget) kcz = (kcz + 1) / 2;
-  // prefer an even split of ns
-  int nkz = (ns + kcz - 1) / kcz;
-  kcz = (ns + nkz - 1) / nkz;
-  g.kcz = kcz;
-  g.nkz = nkz;
-  // threads: enough for every butterfly of the widest stage, a multiple of 32, at most 512
+  // butterflies per line in the widest stage; threads along y of every block
   int minr = 8;
   for (int i = 0; i < plan.nst; ++i) minr = plan.radix[i] < minr ? plan.radix[i] : minr;
-  auto threads = [&](int lines) {
-    int t = lines * (n / minr);
-    t = (t + 31) / 32 * 32;
-    return t < 64 ? 64 : (t > 512 ? 512 : t);
+  const int nb = n / minr;
+  auto by_for = [&](int lines) {
+    int by = nb;
+    while (by > 1 && lines * by > 512) by = (by + 1) / 2;
+    return by;
   };
-  g.thr_x = threads(3 * g.rb / 2);
-  g.thr_y = threads(g.kcy);
-  g.thr_z = threads(3 * g.kcz) > 256 ? 256 : threads(3 * g.kcz);
+  // x passes: rb rows (z,y) -> 3 rb / 2 complex lines, rb | n*n, at most ~48 lines
+  int rb = 16;
+  while (rb > 2 && ((size_t(n) * n) % rb != 0 || 2 * (3 * size_t(rb) / 2) * line > kFFTSmemBudget ||
+                    3 * rb / 2 > 512))
+    rb /= 2;
+  g.rb = rb;
+  // y passes: kcy kx columns per block (one line per x-thread)
+  int nky = 1;
+  while ((ns + nky - 1) / nky > 64 || 2 * size_t((ns + nky - 1) / nky) * line > kFFTSmemBudget) ++nky;
+  g.nky = nky;
+  g.kcy = (ns + nky - 1) / nky;
+  // z pass: 3 components x kcz columns per block
+  int nkz = 1;
+  while (3 * ((ns + nkz - 1) / nkz) > 48 || 2 * 3 * size_t((ns + nkz - 1) / nkz) * line > kFFTSmemBudget) ++nkz;
+  g.nkz = nkz;
+  g.kcz = (ns + nkz - 1) / nkz;
+  g.by_x = by_for(3 * g.rb / 2);
+  g.by_y = by_for(g.kcy);
+  g.by_z = by_for(3 * g.kcz);
+  g.thr_x = 3 * g.rb / 2 * g.by_x;
+  g.thr_y = g.kcy * g.by_y;
+  g.thr_z = 3 * g.kcz * g.by_z;
+  g.div_3n = make_fastdiv(unsigned(3 * n));
+  g.div_ns = make_fastdiv(unsigned(ns));
+  g.div_n = make_fastdiv(unsigned(n));
+  g.div_kcz = make_fastdiv(unsigned(g.kcz));
   return g;
 }
 
@@ -144,20 +157,21 @@ template <typename T> struct Radix<T, 5> {
   }
 };
 
-// One Stockham stage over `nlines` lines of length n (pitch `pitch`): out[(j/Ns)Ns R + j%Ns + r Ns] =
-// DFT_R over r of in[j + r n/R] * W^{r (j%Ns)}, W = e^{-2 pi i/(Ns R)}.
+// One Stockham stage on the line owned by this thread (line < 0: idle thread), butterflies j along
+// threadIdx.y: out[(j/Ns)Ns R + j%Ns + r Ns] = DFT_R over r of in[j + r n/R] * W^{r (j%Ns)},
+// W = e^{-2 pi i/(Ns R)}.
 template <typename T, int R>
-__device__ __forceinline__ void stage(const cplx<T>* __restrict__ src, cplx<T>* __restrict__ dst, int nlines, int pitch,
-                                      int n, int Ns, const cplx<T>* __restrict__ tw, bool inv, int tid, int nthr) {
+__device__ __forceinline__ void stage(const cplx<T>* __restrict__ src, cplx<T>* __restrict__ dst, int line, int pitch,
+                                      int n, int Ns, const FastDiv& nsd, const cplx<T>* __restrict__ tw, bool inv) {
   using C = cplx<T>;
+  if (line < 0) return;
   const int nb = n / R;
-  const int total = nlines * nb;
   const int step = n / (Ns * R);
-  for (int k = tid; k < total; k += nthr) {
-    const int line = k % nlines, j = k / nlines;
-    const C* s = src + line * pitch;
-    C* d = dst + line * pitch;
-    const int jm = j % Ns;
+  const C* s = src + line * pitch;
+  C* d = dst + line * pitch;
+  for (int j = threadIdx.y; j < nb; j += blockDim.y) {
+    const int jq = fdiv(j, nsd);
+    const int jm = j - jq * Ns;
     C v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = s[j + r * nb];
@@ -170,27 +184,28 @@ __device__ __forceinline__ void stage(const cplx<T>* __restrict__ src, cplx<T>* 
       }
     }
     Radix<T, R>::run(v, inv);
-    const int base = (j - jm) * R + jm;
+    const int base = jq * Ns * R + jm;
 #pragma unroll
     for (int r = 0; r < R; ++r) d[base + r * Ns] = v[r];
   }
 }
 
-// Runs all stages; returns the buffer holding the result.
+// Runs all stages on the thread's line; returns the buffer holding the result.
 template <typename T>
-__device__ cplx<T>* fft_lines(cplx<T>* b0, cplx<T>* b1, int nlines, int pitch, const FFTPlan& pl,
-                              const cplx<T>* tw, bool inv, int tid, int nthr) {
+__device__ cplx<T>* fft_lines(cplx<T>* b0, cplx<T>* b1, int line, int pitch, const FFTPlan& pl, const cplx<T>* tw,
+                              bool inv) {
   cplx<T>* src = b0;
   cplx<T>* dst = b1;
   int Ns = 1;
   for (int st = 0; st < pl.nst; ++st) {
     const int R = pl.radix[st];
+    const FastDiv& nsd = pl.ns_div[st];
     switch (R) {
-      case 8: stage<T, 8>(src, dst, nlines, pitch, pl.n, Ns, tw, inv, tid, nthr); break;
-      case 4: stage<T, 4>(src, dst, nlines, pitch, pl.n, Ns, tw, inv, tid, nthr); break;
-      case 2: stage<T, 2>(src, dst, nlines, pitch, pl.n, Ns, tw, inv, tid, nthr); break;
-      case 3: stage<T, 3>(src, dst, nlines, pitch, pl.n, Ns, tw, inv, tid, nthr); break;
-      default: stage<T, 5>(src, dst, nlines, pitch, pl.n, Ns, tw, inv, tid, nthr); break;
+      case 8: stage<T, 8>(src, dst, line, pitch, pl.n, Ns, nsd, tw, inv); break;
+      case 4: stage<T, 4>(src, dst, line, pitch, pl.n, Ns, nsd, tw, inv); break;
+      case 2: stage<T, 2>(src, dst, line, pitch, pl.n, Ns, nsd, tw, inv); break;
+      case 3: stage<T, 3>(src, dst, line, pitch, pl.n, Ns, nsd, tw, inv); break;
+      default: stage<T, 5>(src, dst, line, pitch, pl.n, Ns, nsd, tw, inv); break;
     }
     __syncthreads();
     cplx<T>* t = src; src = dst; dst = t;
@@ -222,6 +237,7 @@ __device__ __forceinline__ bool load_on(const GreenArgs& A, int load) {
 }
 
 // ---------------------------------------------------------------------------- FX
+// block (3 rb/2 lines, by): rows (z,y) row0..row0+rb of one load; two real rows per complex line.
 template <typename T>
 __global__ void __launch_bounds__(512) k_fx(const GreenArgs A) {
   using C = cplx<T>;
@@ -229,7 +245,7 @@ __global__ void __launch_bounds__(512) k_fx(const GreenArgs A) {
   const int load = blockIdx.y;
   if (!load_on(A, load)) return;
   const int n = A.n, ns = A.ns, rb = A.geo.rb, pitch = n + 1;
-  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int tid = flat_tid(), nthr = block_threads();
   const int nl = 3 * rb / 2;  // complex lines
   C* b0 = reinterpret_cast<C*>(smem_raw);
   C* b1 = b0 + nl * pitch;
@@ -237,28 +253,29 @@ __global__ void __launch_bounds__(512) k_fx(const GreenArgs A) {
   const size_t row0 = size_t(blockIdx.x) * rb;
   const T* r = reinterpret_cast<const T*>(A.r) + size_t(load) * 3 * N;
   const double* sc = A.scale;
-  double m[3] = {0.0, 0.0, 0.0};
-  if (A.use_mean) { m[0] = A.scal[load].mean_r[0]; m[1] = A.scal[load].mean_r[1]; m[2] = A.scal[load].mean_r[2]; }
+  T m[3] = {T(0), T(0), T(0)};
+  if (A.use_mean) { m[0] = T(A.scal[load].mean_r[0]); m[1] = T(A.scal[load].mean_r[1]); m[2] = T(A.scal[load].mean_r[2]); }
   const int total = rb * 3 * n;
   const size_t gbase = row0 * n * 3;
   for (int i = tid; i < total; i += nthr) {
-    const int rl = i / (3 * n);
+    const int rl = fdiv(i, A.geo.div_3n);
     const int rem = i - rl * 3 * n;
-    const int x = rem / 3, c = rem - 3 * (rem / 3);
+    const int x = rem / 3, c = rem - 3 * x;
     const size_t g = gbase + i;
-    const T v = T(sc[g]) * (r[g] - T(m[c]));
+    const T mc = c == 0 ? m[0] : (c == 1 ? m[1] : m[2]);
+    const T v = T(sc[g]) * (r[g] - mc);
     const int rho = 3 * rl + c;
     T* dst = reinterpret_cast<T*>(b0 + (rho >> 1) * pitch + x);
     dst[rho & 1] = v;
   }
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_lines<T>(b0, b1, nl, pitch, A.plan, tw, false, tid, nthr);
+  C* res = fft_lines<T>(b0, b1, threadIdx.x, pitch, A.plan, tw, false);
   // split: line rho=2l (real part) and rho=2l+1 (imaginary part)
   C* spec = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * size_t(n) * n * ns;
   const int tot2 = 3 * rb * ns;
   for (int i = tid; i < tot2; i += nthr) {
-    const int rho = i / ns, k = i - rho * ns;
+    const int rho = fdiv(i, A.geo.div_ns), k = i - rho * ns;
     const int l = rho >> 1;
     const C zk = res[l * pitch + k];
     const C zn = res[l * pitch + (k == 0 ? 0 : n - k)];
@@ -274,6 +291,7 @@ __global__ void __launch_bounds__(512) k_fx(const GreenArgs A) {
 }
 
 // ---------------------------------------------------------------------------- FY / IFY
+// block (kcy lines, by): one (load, component, z) plane, kx columns k0..k0+kcy.
 template <typename T, bool INV>
 __global__ void __launch_bounds__(512) k_fy(const GreenArgs A) {
   using C = cplx<T>;
@@ -285,25 +303,21 @@ __global__ void __launch_bounds__(512) k_fy(const GreenArgs A) {
   const int z = blockIdx.y;
   const int k0 = blockIdx.x * kc;
   const int kn = min(kc, ns - k0);
-  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int kl = threadIdx.x;
   C* b0 = reinterpret_cast<C*>(smem_raw);
   C* b1 = b0 + kc * pitch;
   C* plane = reinterpret_cast<C*>(A.spec) + (size_t(load) * 3 + c) * size_t(n) * n * ns + size_t(z) * n * ns;
-  const int total = n * kn;
-  for (int i = tid; i < total; i += nthr) {
-    const int y = i / kn, kl = i - y * kn;
-    b0[kl * pitch + y] = plane[size_t(y) * ns + k0 + kl];
-  }
+  if (kl < kn)
+    for (int y = threadIdx.y; y < n; y += blockDim.y) b0[kl * pitch + y] = plane[size_t(y) * ns + k0 + kl];
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_lines<T>(b0, b1, kn, pitch, A.plan, tw, INV, tid, nthr);
-  for (int i = tid; i < total; i += nthr) {
-    const int y = i / kn, kl = i - y * kn;
-    plane[size_t(y) * ns + k0 + kl] = res[kl * pitch + y];
-  }
+  C* res = fft_lines<T>(b0, b1, kl < kn ? kl : -1, pitch, A.plan, tw, INV);
+  if (kl < kn)
+    for (int y = threadIdx.y; y < n; y += blockDim.y) plane[size_t(y) * ns + k0 + kl] = res[kl * pitch + y];
 }
 
 // ---------------------------------------------------------------------------- FZ (+ symbol)
+// block (kcz, by, 3): one (load, ky), kx columns k0..k0+kcz, the three components along z.
 template <typename T>
 __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
   using C = cplx<T>;
@@ -314,52 +328,50 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
   const int ky = blockIdx.y;
   const int k0 = blockIdx.x * kc;
   const int kn = min(kc, ns - k0);
-  const int tid = threadIdx.x, nthr = blockDim.x;
-  const int nl = 3 * kn;
+  const int kl = threadIdx.x, c = threadIdx.z;
+  const int tid = flat_tid();
   C* b0 = reinterpret_cast<C*>(smem_raw);
   C* b1 = b0 + 3 * kc * pitch;
   double* red = reinterpret_cast<double*>(b1 + 3 * kc * pitch);
   const size_t plane = size_t(n) * n * ns;  // one component
   C* sp = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * plane;
-  const int total = 3 * n * kn;
-  for (int i = tid; i < total; i += nthr) {
-    const int kl = i % kn, t = i / kn, z = t % n, c = t / n;
-    b0[(c * kn + kl) * pitch + z] = sp[c * plane + (size_t(z) * n + ky) * ns + k0 + kl];
-  }
+  const int line = c * kc + kl;
+  if (kl < kn)
+    for (int z = threadIdx.y; z < n; z += blockDim.y)
+      b0[line * pitch + z] = sp[c * plane + (size_t(z) * n + ky) * ns + k0 + kl];
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_lines<T>(b0, b1, nl, pitch, A.plan, tw, false, tid, nthr);
-  // symbol multiply and Parseval partial sum
+  C* res = fft_lines<T>(b0, b1, kl < kn ? line : -1, pitch, A.plan, tw, false);
+  // symbol multiply and Parseval partial sum: rows kz over (threadIdx.y, threadIdx.z)
   const T* sym = reinterpret_cast<const T*>(A.sym);
   const size_t Nh = size_t(n) * n * ns;
   double acc[1] = {0.0};
-  const int tot2 = n * kn;
-  for (int i = tid; i < tot2; i += nthr) {
-    const int kl = i % kn, kz = i / kn;
+  if (kl < kn) {
     const int kx = k0 + kl;
-    const size_t kk = (size_t(kz) * n + ky) * ns + kx;
-    const T c0 = sym[kk], c1 = sym[Nh + kk], c2 = sym[2 * Nh + kk];
-    const T c3 = sym[3 * Nh + kk], c4 = sym[4 * Nh + kk], c5 = sym[5 * Nh + kk];
-    C* px = res + (0 * kn + kl) * pitch + kz;
-    C* py = res + (1 * kn + kl) * pitch + kz;
-    C* pz = res + (2 * kn + kl) * pitch + kz;
-    const C x = *px, y = *py, z = *pz;
-    C wx, wy, wz;
-    wx.x = c0 * x.x + c3 * y.x + c4 * z.x; wx.y = c0 * x.y + c3 * y.y + c4 * z.y;
-    wy.x = c3 * x.x + c1 * y.x + c5 * z.x; wy.y = c3 * x.y + c1 * y.y + c5 * z.y;
-    wz.x = c4 * x.x + c5 * y.x + c2 * z.x; wz.y = c4 * x.y + c5 * y.y + c2 * z.y;
     const double wgt = (kx == 0 || kx == n / 2) ? 1.0 : 2.0;
-    acc[0] += wgt * (double(x.x) * wx.x + double(x.y) * wx.y + double(y.x) * wy.x + double(y.y) * wy.y +
-                     double(z.x) * wz.x + double(z.y) * wz.y);
-    *px = wx; *py = wy; *pz = wz;
+    for (int kz = threadIdx.y + blockDim.y * threadIdx.z; kz < n; kz += blockDim.y * blockDim.z) {
+      const size_t kk = (size_t(kz) * n + ky) * ns + kx;
+      const T c0 = sym[kk], c1 = sym[Nh + kk], c2 = sym[2 * Nh + kk];
+      const T c3 = sym[3 * Nh + kk], c4 = sym[4 * Nh + kk], c5 = sym[5 * Nh + kk];
+      C* px = res + (0 * kc + kl) * pitch + kz;
+      C* py = res + (1 * kc + kl) * pitch + kz;
+      C* pz = res + (2 * kc + kl) * pitch + kz;
+      const C x = *px, y = *py, zv = *pz;
+      C wx, wy, wz;
+      wx.x = c0 * x.x + c3 * y.x + c4 * zv.x; wx.y = c0 * x.y + c3 * y.y + c4 * zv.y;
+      wy.x = c3 * x.x + c1 * y.x + c5 * zv.x; wy.y = c3 * x.y + c1 * y.y + c5 * zv.y;
+      wz.x = c4 * x.x + c5 * y.x + c2 * zv.x; wz.y = c4 * x.y + c5 * y.y + c2 * zv.y;
+      acc[0] += wgt * (double(x.x) * wx.x + double(x.y) * wx.y + double(y.x) * wy.x + double(y.y) * wy.y +
+                       double(zv.x) * wz.x + double(zv.y) * wz.y);
+      *px = wx; *py = wy; *pz = wz;
+    }
   }
   __syncthreads();
   C* other = (res == b0) ? b1 : b0;
-  C* res2 = fft_lines<T>(res, other, nl, pitch, A.plan, tw, true, tid, nthr);
-  for (int i = tid; i < total; i += nthr) {
-    const int kl = i % kn, t = i / kn, z = t % n, c = t / n;
-    sp[c * plane + (size_t(z) * n + ky) * ns + k0 + kl] = res2[(c * kn + kl) * pitch + z];
-  }
+  C* res2 = fft_lines<T>(res, other, kl < kn ? line : -1, pitch, A.plan, tw, true);
+  if (kl < kn)
+    for (int z = threadIdx.y; z < n; z += blockDim.y)
+      sp[c * plane + (size_t(z) * n + ky) * ns + k0 + kl] = res2[line * pitch + z];
   if (!A.finalize_fz) return;
   block_sum<1>(acc, red);
   const int nblk = gridDim.x * gridDim.y, blk = blockIdx.x + gridDim.x * blockIdx.y;
@@ -382,6 +394,7 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
 }
 
 // ---------------------------------------------------------------------------- IFX
+// block (3 rb/2 lines, by): C2R of rb rows, two rows per complex line; s.w and its sums.
 template <typename T>
 __global__ void __launch_bounds__(512) k_ifx(const GreenArgs A) {
   using C = cplx<T>;
@@ -389,7 +402,7 @@ __global__ void __launch_bounds__(512) k_ifx(const GreenArgs A) {
   const int load = blockIdx.y;
   if (!load_on(A, load)) return;
   const int n = A.n, ns = A.ns, rb = A.geo.rb, pitch = n + 1;
-  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int tid = flat_tid(), nthr = block_threads();
   const int nl = 3 * rb / 2;
   C* b0 = reinterpret_cast<C*>(smem_raw);
   C* b1 = b0 + nl * pitch;
@@ -400,7 +413,7 @@ __global__ void __launch_bounds__(512) k_ifx(const GreenArgs A) {
   // Z[k] = A[k] + i B[k] over the full line, A/B Hermitian-extended; DC/Nyquist imaginary parts dropped
   const int total = nl * n;
   for (int i = tid; i < total; i += nthr) {
-    const int l = i / n, k = i - l * n;
+    const int l = fdiv(i, A.geo.div_n), k = i - l * n;
     C v[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
@@ -423,22 +436,25 @@ __global__ void __launch_bounds__(512) k_ifx(const GreenArgs A) {
   }
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_lines<T>(b0, b1, nl, pitch, A.plan, tw, true, tid, nthr);
+  C* res = fft_lines<T>(b0, b1, threadIdx.x, pitch, A.plan, tw, true);
   T* sw = reinterpret_cast<T*>(A.sw) + size_t(load) * 3 * N;
   const double* sc = A.scale;
   double acc[3] = {0.0, 0.0, 0.0};
   const int tot2 = rb * 3 * n;
   const size_t gbase = row0 * n * 3;
   for (int i = tid; i < tot2; i += nthr) {
-    const int rl = i / (3 * n);
+    const int rl = fdiv(i, A.geo.div_3n);
     const int rem = i - rl * 3 * n;
-    const int x = rem / 3, c = rem - 3 * (rem / 3);
+    const int x = rem / 3, c = rem - 3 * x;
     const int rho = 3 * rl + c;
     const C zz = res[(rho >> 1) * pitch + x];
     const T w = (rho & 1) ? zz.y : zz.x;
     const T o = T(sc[gbase + i]) * w;
     sw[gbase + i] = o;
-    acc[c] += double(o);
+    const double od = double(o);
+    acc[0] += c == 0 ? od : 0.0;
+    acc[1] += c == 1 ? od : 0.0;
+    acc[2] += c == 2 ? od : 0.0;
   }
   block_sum<3>(acc, red);
   const int nblk = gridDim.x;
@@ -485,11 +501,11 @@ static int run_green_pass(pgj_ctx* c, int loads, GreenArgs& A, cudaStream_t s, i
   const int n = c->n;
   const FFTGeom& g = c->fg;
   switch (pass) {
-    case 0: k_fx<T><<<dim3((n * n) / g.rb, loads), g.thr_x, smem_x(c, cb), s>>>(A); break;
-    case 1: k_fy<T, false><<<dim3(g.nky, n, 3 * loads), g.thr_y, smem_y(c, cb), s>>>(A); break;
-    case 2: k_fz<T><<<dim3(g.nkz, n, loads), g.thr_z, smem_z(c, cb), s>>>(A); break;
-    case 3: k_fy<T, true><<<dim3(g.nky, n, 3 * loads), g.thr_y, smem_y(c, cb), s>>>(A); break;
-    default: k_ifx<T><<<dim3((n * n) / g.rb, loads), g.thr_x, smem_x(c, cb), s>>>(A); break;
+    case 0: k_fx<T><<<dim3((n * n) / g.rb, loads), dim3(3 * g.rb / 2, g.by_x), smem_x(c, cb), s>>>(A); break;
+    case 1: k_fy<T, false><<<dim3(g.nky, n, 3 * loads), dim3(g.kcy, g.by_y), smem_y(c, cb), s>>>(A); break;
+    case 2: k_fz<T><<<dim3(g.nkz, n, loads), dim3(g.kcz, g.by_z, 3), smem_z(c, cb), s>>>(A); break;
+    case 3: k_fy<T, true><<<dim3(g.nky, n, 3 * loads), dim3(g.kcy, g.by_y), smem_y(c, cb), s>>>(A); break;
+    default: k_ifx<T><<<dim3((n * n) / g.rb, loads), dim3(3 * g.rb / 2, g.by_x), smem_x(c, cb), s>>>(A); break;
   }
   return check_launch();
 }

@@ -11,6 +11,7 @@ struct FFTPlan {
   int n;
   int nst;
   int radix[kMaxStages];
+  FastDiv ns_div[kMaxStages];  // stride Ns of each stage (product of the earlier radices)
 };
 bool make_fft_plan(int n, FFTPlan* plan);
 
@@ -32,7 +33,9 @@ struct FFTGeom {
   int nky;       // y-pass chunks
   int kcz;       // kx columns per z-pass block
   int nkz;       // z-pass chunks
-  int thr_x, thr_y, thr_z;  // threads per block of the x, y and z passes (>= butterflies of a stage)
+  int thr_x, thr_y, thr_z;  // threads per block of the x, y and z passes
+  int by_x, by_y, by_z;     // threads along y (butterflies of a line) per pass; x (and z) index lines
+  FastDiv div_3n, div_ns, div_n, div_kcz;
 };
 FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan);
 
