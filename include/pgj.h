@@ -115,6 +115,13 @@ int pgj_green_symbol(int n, double lam, double mu, double* symbol, void* stream)
  * certificate and the stopping rule are the FP64 ones. */
 int pgj_solve(pgj_ctx* ctx, int loads, const double* macros, double rtol, double* u,
               pgj_load_info* info, void* stream);
+/* Enqueue the same certified solve on `stream` without any host synchronisation: the restarts of
+ * resident.py:194-205 are decided on the device (a graph WHILE node), so the whole solve is one
+ * graph launch. Several contexts on several streams therefore run concurrently. Complete it with
+ * pgj_solve_wait, which synchronises `stream` once and fills `info`. Not available for mixed mode 1
+ * (PGJ_ERR_UNSUPPORTED). */
+int pgj_solve_async(pgj_ctx* ctx, int loads, const double* macros, double rtol, double* u, void* stream);
+int pgj_solve_wait(pgj_ctx* ctx, pgj_load_info* info, void* stream);
 /* Inner relative tolerance of the FP32 refinement sweeps (mode 1; default 1e-5). */
 int pgj_set_inner_rtol(pgj_ctx* ctx, double inner_rtol);
 /* Mixed-precision scheme of a PGJ_FP32 context (no reference counterpart: the reference is FP64 only).

@@ -59,6 +59,8 @@ SIGNATURES = {
     "pgj_precondition": (C.c_int, [vp, C.c_int, vp, vp, vp]),
     "pgj_green_symbol": (C.c_int, [C.c_int, f64, f64, vp, vp]),
     "pgj_solve": (C.c_int, [vp, C.c_int, vp, f64, vp, C.POINTER(LoadInfo), vp]),
+    "pgj_solve_async": (C.c_int, [vp, C.c_int, vp, f64, vp, vp]),
+    "pgj_solve_wait": (C.c_int, [vp, C.POINTER(LoadInfo), vp]),
     "pgj_set_inner_rtol": (C.c_int, [vp, f64]),
     "pgj_set_mixed_mode": (C.c_int, [vp, C.c_int, f64]),
     "pgj_last_refinements": (C.c_int, [vp]),

@@ -23,13 +23,19 @@ int set_cuda_error(cudaError_t e) {
 
 struct Graphs {
   cudaStream_t cap = nullptr;  // private capture stream
-  int loads = 0;
+  int loads = 0;          // solve graph
+  int attempt_loads = 0;  // certification / attempt graphs
+  int attempt_mode = -1;
   double inner_rtol = 0.0;
   cudaGraphExec_t cert = nullptr;
   cudaGraphExec_t attempt = nullptr;  // FP64: init + PCG loop + certify; mixed: one refinement sweep
+  cudaGraphExec_t solve = nullptr;    // whole certified solve with device-side restarts
+  double rtol = 0.0;
+  int mode = -1;
   ~Graphs() {
     if (cert) cudaGraphExecDestroy(cert);
     if (attempt) cudaGraphExecDestroy(attempt);
+    if (solve) cudaGraphExecDestroy(solve);
     if (cap) cudaStreamDestroy(cap);
   }
 };
@@ -214,25 +220,10 @@ static int capture_pcg(pgj_ctx* c, int L, cudaStream_t s, bool reliable = false)
   return st;
 }
 
-static int build_graphs(pgj_ctx* c, int L) {
-  Graphs* G = c->graphs;
-  if (G->loads == L && G->cert && G->attempt && G->inner_rtol == c->inner_rtol) return PGJ_OK;
-  if (G->cert) { cudaGraphExecDestroy(G->cert); G->cert = nullptr; }
-  if (G->attempt) { cudaGraphExecDestroy(G->attempt); G->attempt = nullptr; }
-  cudaStream_t s = G->cap;
-  cudaGraph_t g = nullptr;
+// One attempt: FP64 -> init masks, PCG loop, certify; mixed reliable -> FP32 recurrence with
+// true-residual replacements, fold, certify; mixed sweeps -> one refinement sweep.
+static int capture_attempt(pgj_ctx* c, int L, cudaStream_t s) {
   int st;
-  cudaError_t e;
-  // certification graph
-  if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return set_cuda_error(e);
-  st = capture_cert(c, L, s);
-  if ((st = end_capture(s, &g, st))) return st;
-  e = cudaGraphInstantiate(&G->cert, g, 0);
-  cudaGraphDestroy(g);
-  if (e != cudaSuccess) return set_cuda_error(e);
-  // FP64 attempt: init masks -> PCG loop -> certify.
-  // Mixed sweep: r_in = T(r64), d = 0 -> inner PCG loop (FP32) -> x += d -> FP64 certify.
-  if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return set_cuda_error(e);
   if (c->prec == PGJ_FP32 && c->mixed_mode == 0) {
     st = launch_rel_start(c, L, s);
     if (!st) {
@@ -254,11 +245,70 @@ static int build_graphs(pgj_ctx* c, int L) {
     if (!st) st = capture_pcg(c, L, s);
   }
   if (!st) st = capture_cert(c, L, s);
+  return st;
+}
+
+// Whole certified solve as one graph (FP64 and mixed reliable-update modes):
+// counters <- 0; f = rhs(macros); targets; certify; WHILE(restart){attempt; decide}.
+static int build_solve_graph(pgj_ctx* c, int L, double rtol) {
+  Graphs* G = c->graphs;
+  if (G->solve && G->loads == L && G->rtol == rtol && G->mode == c->mixed_mode) return PGJ_OK;
+  if (G->solve) { cudaGraphExecDestroy(G->solve); G->solve = nullptr; }
+  cudaStream_t s = G->cap;
+  cudaGraph_t g = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  int st = PGJ_OK;
+  c->scal = c->scal_out;
+  if ((e = cudaMemsetAsync(c->cond, 0, 8 * sizeof(int), s)) != cudaSuccess) st = set_cuda_error(e);
+  if (!st) st = launch_rhs(c, L, c->macros, c->f, s);
+  if (!st) st = launch_norms(c, L, c->f, rtol, s);
+  if (!st) st = capture_cert(c, L, s);
+  cudaGraphConditionalHandle h = 0;
+  cudaGraph_t body = nullptr;
+  if (!st) st = add_conditional(s, &h, 1, cudaGraphCondTypeWhile, &body);
+  if (!st)
+    st = capture_into(body, [&](cudaStream_t s2) {
+      int r = capture_attempt(c, L, s2);
+      return r ? r : launch_decide(c, L, h, s2);
+    });
+  if ((st = end_capture(s, &g, st))) return st;
+  e = cudaGraphInstantiate(&G->solve, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  G->loads = L;
+  G->rtol = rtol;
+  G->mode = c->mixed_mode;
+  return PGJ_OK;
+}
+
+static int build_graphs(pgj_ctx* c, int L) {
+  Graphs* G = c->graphs;
+  if (G->attempt_loads == L && G->cert && G->attempt && G->inner_rtol == c->inner_rtol &&
+      G->attempt_mode == c->mixed_mode)
+    return PGJ_OK;
+  if (G->cert) { cudaGraphExecDestroy(G->cert); G->cert = nullptr; }
+  if (G->attempt) { cudaGraphExecDestroy(G->attempt); G->attempt = nullptr; }
+  cudaStream_t s = G->cap;
+  cudaGraph_t g = nullptr;
+  int st;
+  cudaError_t e;
+  // certification graph
+  if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return set_cuda_error(e);
+  st = capture_cert(c, L, s);
+  if ((st = end_capture(s, &g, st))) return st;
+  e = cudaGraphInstantiate(&G->cert, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  // one attempt (see capture_attempt)
+  if ((e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal)) != cudaSuccess) return set_cuda_error(e);
+  st = capture_attempt(c, L, s);
   if ((st = end_capture(s, &g, st))) return st;
   e = cudaGraphInstantiate(&G->attempt, g, 0);
   cudaGraphDestroy(g);
   if (e != cudaSuccess) return set_cuda_error(e);
-  G->loads = L;
+  G->attempt_loads = L;
+  G->attempt_mode = c->mixed_mode;
   G->inner_rtol = c->inner_rtol;
   return PGJ_OK;
 }
@@ -362,6 +412,7 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) st = set_cuda_error(e);
   }
+  if (!st) st = launch_scale(c, 0.5, s);  // stages the diagonal constants (once)
   if (!st) st = launch_scale(c, 0.0, s);  // scale = 1 until an alpha is selected
   if (!st) st = autotune_stencil(c, s);
   if (st) {
@@ -407,11 +458,18 @@ int pgj_apply_f32(pgj_ctx* c, int loads, const float* p, const int32_t* active, 
   return launch_stencil(c, kPlain, loads, PGJ_FP32, p, q, nullptr, active, static_cast<cudaStream_t>(stream));
 }
 
+// Copies the (loads, 6) macro strains to the device unless the same values are already there
+// (a pageable host-to-device copy serialises the stream, so repeated solves skip it).
 static int stage_macros(pgj_ctx* c, int loads, const double* macros, cudaStream_t s) {
   for (int i = 0; i < 6 * loads; ++i)
     if (!std::isfinite(macros[i])) return PGJ_ERR_NONFINITE;
+  if (c->staged_loads >= loads && std::memcmp(c->staged_macros, macros, sizeof(double) * 6 * size_t(loads)) == 0)
+    return PGJ_OK;
   cudaError_t e = cudaMemcpyAsync(c->macros, macros, sizeof(double) * 6 * size_t(loads), cudaMemcpyHostToDevice, s);
-  return e == cudaSuccess ? PGJ_OK : set_cuda_error(e);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  std::memcpy(c->staged_macros, macros, sizeof(double) * 6 * size_t(loads));
+  c->staged_loads = loads;
+  return PGJ_OK;
 }
 
 int pgj_rhs(pgj_ctx* c, int loads, const double* macros, double* f, void* stream) {
@@ -446,6 +504,7 @@ int pgj_set_mixed_mode(pgj_ctx* c, int mode, double delta) {
   c->mixed_mode = mode;
   c->rel_delta2 = c->prec == PGJ_FP32 ? delta * delta : 0.0;
   c->graphs->loads = 0;  // rebuild the solve graphs with the new scheme
+  c->graphs->attempt_loads = 0;
   return PGJ_OK;
 }
 
@@ -453,8 +512,66 @@ int pgj_set_mixed_mode(pgj_ctx* c, int mode, double delta) {
 // inner_rtol relative, x += d, FP64 certification).
 static constexpr int kMaxSweeps = 12;
 
+int pgj_solve_async(pgj_ctx* c, int loads, const double* macros, double rtol, double* u, void* stream) {
+  if (!c || !macros || !u || loads < 1 || loads > c->L || !(rtol > 0)) return PGJ_ERR_ARGUMENT;
+  if (c->prec == PGJ_FP32 && c->mixed_mode == 1) return PGJ_ERR_UNSUPPORTED;  // sweeps need the host
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const size_t bytes = sizeof(double) * 3 * size_t(c->N) * loads;
+  int st = stage_macros(c, loads, macros, s);
+  if (!st) st = build_solve_graph(c, loads, rtol);
+  if (st) return st;
+  cudaError_t e = cudaSuccess;
+  if (u != c->x) e = cudaMemcpyAsync(c->x, u, bytes, cudaMemcpyDeviceToDevice, s);
+  if (e == cudaSuccess) e = cudaGraphLaunch(c->graphs->solve, s);
+  if (e == cudaSuccess && u != c->x) e = cudaMemcpyAsync(u, c->x, bytes, cudaMemcpyDeviceToDevice, s);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  c->pending_loads = loads;
+  return PGJ_OK;
+}
+
+int pgj_solve_wait(pgj_ctx* c, pgj_load_info* info, void* stream) {
+  if (!c || !info || c->pending_loads < 1) return PGJ_ERR_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int loads = c->pending_loads;
+  c->pending_loads = 0;
+  std::vector<LoadScalars> h(loads);
+  int cnt[8] = {0};
+  cudaError_t e = cudaMemcpyAsync(h.data(), c->scal_out, sizeof(LoadScalars) * loads, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, c->cond, sizeof(cnt), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  bool all = true;
+  for (int l = 0; l < loads; ++l) {
+    pgj_load_info& I = info[l];
+    const double thr = std::sqrt(h[l].target2);
+    const bool ok = std::isfinite(h[l].absolute) && h[l].absolute <= thr && h[l].bad == 0;
+    I.rhs_norm = h[l].norm;
+    I.absolute_residual = h[l].absolute;
+    I.threshold = thr;
+    I.relative_residual = h[l].absolute / (h[l].norm > 1e-300 ? h[l].norm : 1e-300);
+    I.iterations = h[l].iterations;
+    I.converged = ok;
+    I.restarts = cnt[4];
+    I.bad = h[l].bad;
+    all = all && ok;
+  }
+  const long long attempts = cnt[4] + 1;
+  if (c->prec == PGJ_FP32)  // rel start, Green, p init, fold, certify, decide; 9 per body; 3 per replacement
+    c->last_launches = 2 + 3 + attempts * (7 + 1 + 3 + 1) + 9LL * cnt[5] + 3LL * cnt[3];
+  else  // init mask, Green, p init, certify, decide; 8 per body
+    c->last_launches = 2 + 3 + attempts * (7 + 3 + 1) + 8LL * cnt[5];
+  c->last_refinements = c->prec == PGJ_FP32 ? 1 + cnt[3] : 1;
+  if (cnt[2]) return PGJ_ERR_TIMEOUT;
+  if (cnt[1]) return PGJ_ERR_ITERATION_CAP;
+  return all ? PGJ_OK : PGJ_ERR_CERTIFICATION;
+}
+
 int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* u, pgj_load_info* info, void* stream) {
   if (!c || !macros || !u || !info || loads < 1 || loads > c->L || !(rtol > 0)) return PGJ_ERR_ARGUMENT;
+  if (!(c->prec == PGJ_FP32 && c->mixed_mode == 1)) {
+    const int st = pgj_solve_async(c, loads, macros, rtol, u, stream);
+    return st ? st : pgj_solve_wait(c, info, stream);
+  }
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const size_t N3 = 3 * size_t(c->N);
   const bool mixed = c->prec == PGJ_FP32 && c->mixed_mode == 1;  // restarted refinement sweeps

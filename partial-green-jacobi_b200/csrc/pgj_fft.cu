@@ -14,6 +14,7 @@
 // Loads whose recurrence is inactive are skipped block-uniformly.
 #include "pgj_internal.h"
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -53,19 +54,24 @@ FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan) {
     while (by > 1 && lines * by > 512) by = (by + 1) / 2;
     return by;
   };
+  // tuning overrides (sweeps): PGJ_FFT_RB rows per x block, PGJ_FFT_NKY / PGJ_FFT_NKZ column chunks
+  auto env = [](const char* k, int dflt) {
+    const char* v = std::getenv(k);
+    return v ? std::atoi(v) : dflt;
+  };
   // x passes: rb rows (z,y) -> 3 rb / 2 complex lines, rb | n*n, at most ~48 lines
-  int rb = 16;
+  int rb = env("PGJ_FFT_RB", 16);
   while (rb > 2 && ((size_t(n) * n) % rb != 0 || 2 * (3 * size_t(rb) / 2) * line > kFFTSmemBudget ||
                     3 * rb / 2 > 512))
     rb /= 2;
   g.rb = rb;
   // y passes: kcy kx columns per block (one line per x-thread)
-  int nky = 1;
+  int nky = env("PGJ_FFT_NKY", 1);
   while ((ns + nky - 1) / nky > 64 || 2 * size_t((ns + nky - 1) / nky) * line > kFFTSmemBudget) ++nky;
   g.nky = nky;
   g.kcy = (ns + nky - 1) / nky;
   // z pass: 3 components x kcz columns per block
-  int nkz = 1;
+  int nkz = env("PGJ_FFT_NKZ", 1);
   while (3 * ((ns + nkz - 1) / nkz) > 48 || 2 * 3 * size_t((ns + nkz - 1) / nkz) * line > kFFTSmemBudget) ++nkz;
   g.nkz = nkz;
   g.kcz = (ns + nkz - 1) / nkz;

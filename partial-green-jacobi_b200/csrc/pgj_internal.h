@@ -116,6 +116,10 @@ struct pgj_ctx {
   double rel_delta2;   // mixed reliable updates: replace r when ||r||^2 < rel_delta2 * anchor (0 = off)
   int mixed_mode;      // 0 reliable-update CG, 1 restarted refinement sweeps
   int last_refinements;
+  int pending_loads;       // loads of the solve enqueued by pgj_solve_async
+  int diag_staged;         // stiffness-diagonal constants copied to aux
+  int staged_loads;        // macros already on the device
+  double staged_macros[6 * 8];
   long long last_launches;
   pgj::Graphs* graphs;
 };
@@ -148,6 +152,7 @@ int launch_inner_start(pgj_ctx* c, int loads, double inner_rtol, cudaStream_t s)
 int launch_inner_finish(pgj_ctx* c, int loads, cudaStream_t s);
 // reliable-update mixed solve (pgj_pcg.cu)
 int launch_rel_start(pgj_ctx* c, int loads, cudaStream_t s);
+int launch_decide(pgj_ctx* c, int loads, cudaGraphConditionalHandle h, cudaStream_t s);
 int launch_rel_cond(pgj_ctx* c, int loads, cudaGraphConditionalHandle h, cudaStream_t s);
 int launch_rel_fold(pgj_ctx* c, int loads, bool all, cudaStream_t s);
 int launch_rel_sync(pgj_ctx* c, int loads, cudaStream_t s);

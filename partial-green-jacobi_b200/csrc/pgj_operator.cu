@@ -665,11 +665,15 @@ int launch_scale(pgj_ctx* c, double alpha, cudaStream_t s) {
     k_fill<<<296, 256, 0, s>>>(count, c->scale, 1.0);
     return check_launch();
   }
-  double ed[24];
-  element_diagonal(c->n, c->lam, c->mu, ed);
-  double* edd = c->aux;  // 24 diagonal entries, staged in the context's aux block
-  cudaError_t e = cudaMemcpyAsync(edd, ed, sizeof(ed), cudaMemcpyHostToDevice, s);
-  if (e != cudaSuccess) return set_cuda_error(e);
+  double* edd = c->aux;  // 24 diagonal entries, staged once in the context's aux block
+  if (!c->diag_staged) {
+    double ed[24];
+    element_diagonal(c->n, c->lam, c->mu, ed);
+    cudaError_t e = cudaMemcpyAsync(edd, ed, sizeof(ed), cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    c->diag_staged = 1;
+  }
   k_logdiag<<<296, 256, 0, s>>>(c->n, c->a, edd, c->scale, c->scal, c->aux + kAuxPartials);
   int st = check_launch();
   if (st) return st;

@@ -134,6 +134,7 @@ __global__ void __launch_bounds__(256) k_update_p(int n, int loads, T* __restric
     int any = 0;
     for (int l = 0; l < loads; ++l) any |= scal[l].active;
     const int runs = ++body_runs[0];
+    body_runs[5] += 1;                             // loop bodies over the whole solve (launch accounting)
     if (runs >= kMaxBodyRuns) body_runs[1] = 1;  // recorded: loop stopped by the bound
     cudaGraphSetConditional(h, (any && runs < kMaxBodyRuns) ? 1u : 0u);
   }
@@ -176,7 +177,7 @@ int launch_update_p(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, 
 // loop-body counter of the attempt.
 __global__ void k_init_mask(int loads, LoadScalars* scal, int cap, int* body_runs) {
   const int l = threadIdx.x;
-  if (l == 0) { body_runs[0] = 0; body_runs[1] = 0; }
+  if (l == 0) body_runs[0] = 0;
   if (l >= loads) return;
   LoadScalars& S = scal[l];
   S.active = (S.res2 > S.target2) && (S.iterations < cap) && !S.bad ? 1 : 0;
@@ -200,7 +201,7 @@ __global__ void __launch_bounds__(256) k_inner_start(int n, const double* __rest
   const int load = blockIdx.y;
   const LoadScalars& O = out_scal[load];
   LoadScalars& S = in_scal[load];
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) { body_runs[0] = 0; body_runs[1] = 0; }
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) body_runs[0] = 0;
   const bool done = isfinite(O.absolute) && O.absolute * O.absolute <= O.target2 && !O.bad;
   if (done) {
     if (blockIdx.x == 0 && threadIdx.x == 0) { S.active = 0; S.touched = 0; S.iterations = 0; }
@@ -284,7 +285,7 @@ __global__ void __launch_bounds__(256) k_rel_start(int n, const double* __restri
                                                    int* body_runs) {
   const size_t N3 = 3 * size_t(n) * n * n;
   const int load = blockIdx.y;
-  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) { body_runs[0] = 0; body_runs[1] = 0; body_runs[3] = 0; }
+  if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) body_runs[0] = 0;
   const size_t off = size_t(load) * N3;
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x) {
     r[off + i] = T(r64[off + i]);
@@ -354,6 +355,29 @@ __global__ void __launch_bounds__(256) k_rel_sync(int n, const double* __restric
     S.active = isfinite(O.res2) && O.res2 > S.target2 && S.iterations < cap && !S.bad ? 1 : 0;
     S.reliable = 0;
   }
+}
+
+// Device-side restart decision after an attempt's certification (resident.py:202-205): another
+// attempt only when some certificate failed, fewer than two restarts were taken, no load latched
+// `bad`, no failing load reached the iteration cap and the loop bound was not hit.
+__global__ void k_decide(int loads, const LoadScalars* out, int* counters, cudaGraphConditionalHandle h, int cap) {
+  if (threadIdx.x != 0) return;
+  bool all = true, anybad = false, capped = false;
+  for (int l = 0; l < loads; ++l) {
+    const LoadScalars& S = out[l];
+    const bool ok = isfinite(S.absolute) && S.absolute * S.absolute <= S.target2 && !S.bad;
+    all = all && ok;
+    anybad = anybad || S.bad;
+    capped = capped || (!ok && S.iterations >= cap);
+  }
+  const bool again = !all && counters[4] < 2 && !anybad && !capped && !counters[1] && !counters[2];
+  if (again) counters[4] += 1;
+  cudaGraphSetConditional(h, again ? 1u : 0u);
+}
+
+int launch_decide(pgj_ctx* c, int loads, cudaGraphConditionalHandle h, cudaStream_t s) {
+  k_decide<<<1, 32, 0, s>>>(loads, c->scal_out, c->cond, h, 4000);
+  return check_launch();
 }
 
 int launch_rel_start(pgj_ctx* c, int loads, cudaStream_t s) {

@@ -315,3 +315,46 @@ def test_profile_iteration_reports_all_kernels(pkg):
         op.set_alpha(0.5)
         prof = op.profile_iteration(np.eye(6), reps=3)
         assert len(prof) == 8 and all(v["ms"] > 0 and v["bytes"] > 0 for v in prof.values())
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_batch_concurrent_designs_match_single_solves(pkg, precision):
+    """Designs of uneven n in flight on separate streams give the single-design results."""
+    lam, mu = pkg.PAPER_MEDIUM
+    designs = [(12, 3, 1e-4, 0.5), (16, 4, 1e-6, 0.25), (12, 5, 1e-9, 1.0), (16, 6, 1e-6, 0.0), (16, 7, 1e-4, 0.75)]
+    reqs = [pkg.Request(torch.tensor(pkg.baseline_design(n, seed, emin)), alpha, tag=i)
+            for i, (n, seed, emin, alpha) in enumerate(designs)]
+    batch = pkg.Batch(slots=2, precision=precision)
+    results = sorted(batch.run(reqs), key=lambda r: r.tag)
+    assert [r.tag for r in results] == list(range(len(designs)))
+    for r, (n, seed, emin, alpha) in zip(results, designs):
+        assert r.status == 0 and all(i["converged"] for i in r.infos)
+        op = pkg.Operator(n, 6, lam, mu)
+        op.set_material(dev(pkg.baseline_design(n, seed, emin)))
+        op.set_alpha(alpha)
+        u = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")
+        _, st = op.solve(np.eye(6), 1e-8, u)
+        assert st == 0
+        C64 = op.effective_tensor(u).cpu().numpy()
+        assert rel(r.C, C64) < (1e-12 if precision == "fp64" else 1e-7), (precision, n, rel(r.C, C64))
+        assert r.latency_ms > 0
+
+
+def test_async_solve_equals_blocking_solve(pkg):
+    n = 16
+    lam, mu = pkg.PAPER_MEDIUM
+    a = dev(pkg.baseline_design(n, 9, 1e-6))
+    op = pkg.Operator(n, 6, lam, mu)
+    op.set_material(a)
+    op.set_alpha(0.5)
+    u1 = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")
+    infos1, st1 = op.solve(np.eye(6), 1e-8, u1)
+    L = pkg._lib.lib()
+    m = np.ascontiguousarray(np.eye(6))
+    u2 = torch.zeros_like(u1)
+    s = torch.cuda.current_stream().cuda_stream
+    pkg._lib.check(L.pgj_solve_async(op._ctx, 6, m.ctypes.data, 1e-8, u2.data_ptr(), s), "async")
+    info = (pkg._lib.LoadInfo * 6)()
+    assert L.pgj_solve_wait(op._ctx, info, s) == 0
+    assert st1 == 0 and [i.iterations for i in info] == [i["iterations"] for i in infos1]
+    assert torch.equal(u1, u2)
