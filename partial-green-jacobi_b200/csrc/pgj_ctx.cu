@@ -46,6 +46,7 @@ static Layout make_layout(int n, int L, int prec) {
   Layout y;
   const size_t N = size_t(n) * n * n, N3 = 3 * N;
   const size_t ns = size_t(n / 2 + 1), Nh = size_t(n) * n * ns;
+  const size_t nsp = ns + (ns & 1);  // spectrum rows padded to an even length (16-byte aligned rows)
   const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t at = o; o = align_up(o + bytes, 256); return at; };
@@ -69,7 +70,7 @@ static Layout make_layout(int n, int L, int prec) {
   y.p = take(tsz * N3 * L);
   y.q = take(tsz * N3 * L);
   y.sw = take(tsz * N3 * L);
-  y.spec = take(2 * tsz * 3 * Nh * L);
+  y.spec = take(2 * tsz * 3 * size_t(n) * n * nsp * L);
   y.total = o;
   return y;
 }

@@ -65,16 +65,21 @@ FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan) {
                     3 * rb / 2 > 512))
     rb /= 2;
   g.rb = rb;
-  // y passes: kcy kx columns per block (one line per x-thread)
+  // y and z passes: tiles of kx columns, an even count so every copied row is 16-byte aligned
+  const int nsp = ns + (ns & 1);
+  auto even_up = [](int v) { return (v + 1) & ~1; };
+  const size_t budget_y = 100 * 1024, budget_z = 120 * 1024;
   int nky = env("PGJ_FFT_NKY", 1);
-  while ((ns + nky - 1) / nky > 64 || 2 * size_t((ns + nky - 1) / nky) * line > kFFTSmemBudget) ++nky;
+  while (nky < nsp && 2 * size_t(n) * even_up((nsp + nky - 1) / nky) * cb > budget_y) ++nky;
   g.nky = nky;
-  g.kcy = (ns + nky - 1) / nky;
-  // z pass: 3 components x kcz columns per block
+  g.kcy = even_up((nsp + nky - 1) / nky);
+  g.nky = (nsp + g.kcy - 1) / g.kcy;
   int nkz = env("PGJ_FFT_NKZ", 1);
-  while (3 * ((ns + nkz - 1) / nkz) > 48 || 2 * 3 * size_t((ns + nkz - 1) / nkz) * line > kFFTSmemBudget) ++nkz;
-  g.nkz = nkz;
-  g.kcz = (ns + nkz - 1) / nkz;
+  while (nkz < nsp && (2 * 3 * size_t(n) * even_up((nsp + nkz - 1) / nkz) * cb > budget_z ||
+                       3 * even_up((nsp + nkz - 1) / nkz) > 512))
+    ++nkz;
+  g.kcz = even_up((nsp + nkz - 1) / nkz);
+  g.nkz = (nsp + g.kcz - 1) / g.kcz;
   g.by_x = by_for(3 * g.rb / 2);
   g.by_y = by_for(g.kcy);
   g.by_z = by_for(3 * g.kcz);
@@ -163,24 +168,21 @@ template <typename T> struct Radix<T, 5> {
   }
 };
 
-// One Stockham stage on the line owned by this thread (line < 0: idle thread), butterflies j along
-// threadIdx.y: out[(j/Ns)Ns R + j%Ns + r Ns] = DFT_R over r of in[j + r n/R] * W^{r (j%Ns)},
-// W = e^{-2 pi i/(Ns R)}.
+// One Stockham stage on the line owned by this thread (its elements at stride es from `src` / `dst`),
+// butterflies j along threadIdx.y: out[(j/Ns)Ns R + j%Ns + r Ns] = DFT_R over r of
+// in[j + r n/R] * W^{r (j%Ns)}, W = e^{-2 pi i/(Ns R)}.
 template <typename T, int R>
-__device__ __forceinline__ void stage(const cplx<T>* __restrict__ src, cplx<T>* __restrict__ dst, int line, int pitch,
-                                      int n, int Ns, const FastDiv& nsd, const cplx<T>* __restrict__ tw, bool inv) {
+__device__ __forceinline__ void stage(const cplx<T>* __restrict__ src, cplx<T>* __restrict__ dst, int es, int n,
+                                      int Ns, const FastDiv& nsd, const cplx<T>* __restrict__ tw, bool inv) {
   using C = cplx<T>;
-  if (line < 0) return;
   const int nb = n / R;
   const int step = n / (Ns * R);
-  const C* s = src + line * pitch;
-  C* d = dst + line * pitch;
   for (int j = threadIdx.y; j < nb; j += blockDim.y) {
     const int jq = fdiv(j, nsd);
     const int jm = j - jq * Ns;
     C v[R];
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = s[j + r * nb];
+    for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * es];
     if (jm) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
@@ -192,26 +194,29 @@ __device__ __forceinline__ void stage(const cplx<T>* __restrict__ src, cplx<T>* 
     Radix<T, R>::run(v, inv);
     const int base = jq * Ns * R + jm;
 #pragma unroll
-    for (int r = 0; r < R; ++r) d[base + r * Ns] = v[r];
+    for (int r = 0; r < R; ++r) dst[(base + r * Ns) * es] = v[r];
   }
 }
 
-// Runs all stages on the thread's line; returns the buffer holding the result.
+// All stages on the thread's line at offset `off` (elements at stride es) of the ping-pong buffers
+// b0/b1; off < 0 marks an idle thread (it still joins the barriers). Returns the result buffer.
 template <typename T>
-__device__ cplx<T>* fft_lines(cplx<T>* b0, cplx<T>* b1, int line, int pitch, const FFTPlan& pl, const cplx<T>* tw,
-                              bool inv) {
+__device__ cplx<T>* fft_line(cplx<T>* b0, cplx<T>* b1, int off, int es, const FFTPlan& pl, const cplx<T>* tw,
+                             bool inv) {
   cplx<T>* src = b0;
   cplx<T>* dst = b1;
   int Ns = 1;
   for (int st = 0; st < pl.nst; ++st) {
     const int R = pl.radix[st];
     const FastDiv& nsd = pl.ns_div[st];
-    switch (R) {
-      case 8: stage<T, 8>(src, dst, line, pitch, pl.n, Ns, nsd, tw, inv); break;
-      case 4: stage<T, 4>(src, dst, line, pitch, pl.n, Ns, nsd, tw, inv); break;
-      case 2: stage<T, 2>(src, dst, line, pitch, pl.n, Ns, nsd, tw, inv); break;
-      case 3: stage<T, 3>(src, dst, line, pitch, pl.n, Ns, nsd, tw, inv); break;
-      default: stage<T, 5>(src, dst, line, pitch, pl.n, Ns, nsd, tw, inv); break;
+    if (off >= 0) {
+      switch (R) {
+        case 8: stage<T, 8>(src + off, dst + off, es, pl.n, Ns, nsd, tw, inv); break;
+        case 4: stage<T, 4>(src + off, dst + off, es, pl.n, Ns, nsd, tw, inv); break;
+        case 2: stage<T, 2>(src + off, dst + off, es, pl.n, Ns, nsd, tw, inv); break;
+        case 3: stage<T, 3>(src + off, dst + off, es, pl.n, Ns, nsd, tw, inv); break;
+        default: stage<T, 5>(src + off, dst + off, es, pl.n, Ns, nsd, tw, inv); break;
+      }
     }
     __syncthreads();
     cplx<T>* t = src; src = dst; dst = t;
@@ -221,7 +226,7 @@ __device__ cplx<T>* fft_lines(cplx<T>* b0, cplx<T>* b1, int line, int pitch, con
 }
 
 struct GreenArgs {
-  int n, ns;
+  int n, ns, nsp;  // grid edge, half-spectrum length, padded (even) spectrum row length
   FFTPlan plan;
   FFTGeom geo;
   const void* r;         // (L,3N) T input residual
@@ -236,6 +241,7 @@ struct GreenArgs {
   int use_mean;          // subtract scal.mean_r before scaling (projection P of the input)
   int init;              // FZ finalizer: initialise rz instead of forming beta
   int finalize_fz;       // FZ last block forms rz / beta (recurrence use only)
+  int* err;              // set to 1 if a bounded device wait expired
 };
 
 __device__ __forceinline__ bool load_on(const GreenArgs& A, int load) {
@@ -276,9 +282,10 @@ __global__ void __launch_bounds__(512) k_fx(const GreenArgs A) {
   }
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_lines<T>(b0, b1, threadIdx.x, pitch, A.plan, tw, false);
+  C* res = fft_line<T>(b0, b1, threadIdx.x * pitch, 1, A.plan, tw, false);
   // split: line rho=2l (real part) and rho=2l+1 (imaginary part)
-  C* spec = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * size_t(n) * n * ns;
+  const int nsp = A.nsp;
+  C* spec = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * size_t(n) * n * nsp;
   const int tot2 = 3 * rb * ns;
   for (int i = tid; i < tot2; i += nthr) {
     const int rho = fdiv(i, A.geo.div_ns), k = i - rho * ns;
@@ -292,12 +299,50 @@ __global__ void __launch_bounds__(512) k_fx(const GreenArgs A) {
       out.x = T(0.5) * (zk.y + zn.y); out.y = T(0.5) * (zn.x - zk.x);
     }
     const int rl = rho / 3, c = rho - 3 * rl;
-    spec[(size_t(c) * n * n + row0 + rl) * ns + k] = out;
+    spec[(size_t(c) * n * n + row0 + rl) * nsp + k] = out;
+  }
+}
+
+// ---------------------------------------------------------------------------- row-tile staging
+// A block's tile is a set of spectrum rows, each `bytes` long and 16-byte aligned, copied with TMA
+// bulk copies into shared memory in their natural layout (row r at r * kcp). One elected warp issues
+// the copies; the block waits on an mbarrier with a bounded poll (timeout -> error flag, early exit).
+template <typename C, typename RowAddr>
+__device__ __forceinline__ bool tile_load(C* dst, int rows, int kcp, unsigned bytes, RowAddr addr, uint64_t* bar,
+                                          int* err) {
+  const int tid = flat_tid();
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid < 32) {
+    if (tid == 0) mbar_expect_tx(bar, bytes * unsigned(rows));
+    __syncwarp();
+    for (int r = tid; r < rows; r += 32) tma_row(dst + size_t(r) * kcp, addr(r), bytes, bar);
+  }
+  const bool ok = mbar_wait(bar, 0);
+  if (__syncthreads_or(!ok)) {
+    if (tid == 0 && err) atomicExch(err, 1);
+    return false;
+  }
+  return true;
+}
+
+template <typename C, typename RowAddr>
+__device__ __forceinline__ void tile_store(const C* src, int rows, int kcp, unsigned bytes, RowAddr addr) {
+  const int tid = flat_tid();
+  fence_proxy_async();
+  __syncthreads();
+  if (tid < 32) {
+    for (int r = tid; r < rows; r += 32) tma_store_row(addr(r), src + size_t(r) * kcp, bytes);
+    tma_store_commit();
+    tma_store_wait_read();
   }
 }
 
 // ---------------------------------------------------------------------------- FY / IFY
-// block (kcy lines, by): one (load, component, z) plane, kx columns k0..k0+kcy.
+// block (kcy lines, by): one (load, component, z) plane, kx columns k0..k0+kcy of every y row.
 template <typename T, bool INV>
 __global__ void __launch_bounds__(512) k_fy(const GreenArgs A) {
   using C = cplx<T>;
@@ -305,49 +350,54 @@ __global__ void __launch_bounds__(512) k_fy(const GreenArgs A) {
   const int lc = blockIdx.z;  // load * 3 + component
   const int load = lc / 3, c = lc - 3 * load;
   if (!load_on(A, load)) return;
-  const int n = A.n, ns = A.ns, pitch = n + 1, kc = A.geo.kcy;
+  const int n = A.n, ns = A.ns, nsp = A.nsp, kc = A.geo.kcy;
   const int z = blockIdx.y;
   const int k0 = blockIdx.x * kc;
-  const int kn = min(kc, ns - k0);
+  const int kn = min(kc, ns - k0);    // live columns
+  const int kcp = min(kc, nsp - k0);  // columns copied (even: 16-byte rows)
   const int kl = threadIdx.x;
   C* b0 = reinterpret_cast<C*>(smem_raw);
-  C* b1 = b0 + kc * pitch;
-  C* plane = reinterpret_cast<C*>(A.spec) + (size_t(load) * 3 + c) * size_t(n) * n * ns + size_t(z) * n * ns;
-  if (kl < kn)
-    for (int y = threadIdx.y; y < n; y += blockDim.y) b0[kl * pitch + y] = plane[size_t(y) * ns + k0 + kl];
-  __syncthreads();
+  C* b1 = b0 + size_t(n) * kc;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(b1 + size_t(n) * kc);
+  C* plane = reinterpret_cast<C*>(A.spec) + (size_t(load) * 3 + c) * size_t(n) * n * nsp + size_t(z) * n * nsp + k0;
+  const unsigned bytes = unsigned(kcp * sizeof(C));
+  if (!tile_load(b0, n, kcp, bytes, [&](int y) { return plane + size_t(y) * nsp; }, bar, A.err)) return;
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_lines<T>(b0, b1, kl < kn ? kl : -1, pitch, A.plan, tw, INV);
-  if (kl < kn)
-    for (int y = threadIdx.y; y < n; y += blockDim.y) plane[size_t(y) * ns + k0 + kl] = res[kl * pitch + y];
+  C* res = fft_line<T>(b0, b1, kl < kn ? kl : -1, kcp, A.plan, tw, INV);
+  tile_store(res, n, kcp, bytes, [&](int y) { return plane + size_t(y) * nsp; });
 }
 
 // ---------------------------------------------------------------------------- FZ (+ symbol)
-// block (kcz, by, 3): one (load, ky), kx columns k0..k0+kcz, the three components along z.
+// block (kcz, by, 3): one (load, ky), kx columns k0..k0+kcz, the three components along z; rows
+// (c, z) of the tile at (c n + z) * kcp.
 template <typename T>
 __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int load = blockIdx.z;
   if (!load_on(A, load)) return;
-  const int n = A.n, ns = A.ns, pitch = n + 1, kc = A.geo.kcz;
+  const int n = A.n, ns = A.ns, nsp = A.nsp, kc = A.geo.kcz;
   const int ky = blockIdx.y;
   const int k0 = blockIdx.x * kc;
   const int kn = min(kc, ns - k0);
+  const int kcp = min(kc, nsp - k0);
   const int kl = threadIdx.x, c = threadIdx.z;
   const int tid = flat_tid();
   C* b0 = reinterpret_cast<C*>(smem_raw);
-  C* b1 = b0 + 3 * kc * pitch;
-  double* red = reinterpret_cast<double*>(b1 + 3 * kc * pitch);
-  const size_t plane = size_t(n) * n * ns;  // one component
-  C* sp = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * plane;
-  const int line = c * kc + kl;
-  if (kl < kn)
-    for (int z = threadIdx.y; z < n; z += blockDim.y)
-      b0[line * pitch + z] = sp[c * plane + (size_t(z) * n + ky) * ns + k0 + kl];
-  __syncthreads();
+  C* b1 = b0 + size_t(3) * n * kc;
+  double* red = reinterpret_cast<double*>(b1 + size_t(3) * n * kc);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(red + 32);
+  const size_t plane = size_t(n) * n * nsp;  // one component
+  C* sp = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * plane + size_t(ky) * nsp + k0;
+  const unsigned bytes = unsigned(kcp * sizeof(C));
+  auto row = [&](int r) {  // r = c * n + z
+    const int cc = r / n, zz = r - cc * n;
+    return sp + cc * plane + size_t(zz) * n * nsp;
+  };
+  if (!tile_load(b0, 3 * n, kcp, bytes, row, bar, A.err)) return;
+  const int off = kl < kn ? c * n * kcp + kl : -1;
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_lines<T>(b0, b1, kl < kn ? line : -1, pitch, A.plan, tw, false);
+  C* res = fft_line<T>(b0, b1, off, kcp, A.plan, tw, false);
   // symbol multiply and Parseval partial sum: rows kz over (threadIdx.y, threadIdx.z)
   const T* sym = reinterpret_cast<const T*>(A.sym);
   const size_t Nh = size_t(n) * n * ns;
@@ -359,9 +409,9 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
       const size_t kk = (size_t(kz) * n + ky) * ns + kx;
       const T c0 = sym[kk], c1 = sym[Nh + kk], c2 = sym[2 * Nh + kk];
       const T c3 = sym[3 * Nh + kk], c4 = sym[4 * Nh + kk], c5 = sym[5 * Nh + kk];
-      C* px = res + (0 * kc + kl) * pitch + kz;
-      C* py = res + (1 * kc + kl) * pitch + kz;
-      C* pz = res + (2 * kc + kl) * pitch + kz;
+      C* px = res + (0 * n + kz) * kcp + kl;
+      C* py = res + (1 * n + kz) * kcp + kl;
+      C* pz = res + (2 * n + kz) * kcp + kl;
       const C x = *px, y = *py, zv = *pz;
       C wx, wy, wz;
       wx.x = c0 * x.x + c3 * y.x + c4 * zv.x; wx.y = c0 * x.y + c3 * y.y + c4 * zv.y;
@@ -374,10 +424,8 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
   }
   __syncthreads();
   C* other = (res == b0) ? b1 : b0;
-  C* res2 = fft_lines<T>(res, other, kl < kn ? line : -1, pitch, A.plan, tw, true);
-  if (kl < kn)
-    for (int z = threadIdx.y; z < n; z += blockDim.y)
-      sp[c * plane + (size_t(z) * n + ky) * ns + k0 + kl] = res2[line * pitch + z];
+  C* res2 = fft_line<T>(res, other, off, kcp, A.plan, tw, true);
+  tile_store(res2, 3 * n, kcp, bytes, row);
   if (!A.finalize_fz) return;
   block_sum<1>(acc, red);
   const int nblk = gridDim.x * gridDim.y, blk = blockIdx.x + gridDim.x * blockIdx.y;
@@ -415,7 +463,8 @@ __global__ void __launch_bounds__(512) k_ifx(const GreenArgs A) {
   double* red = reinterpret_cast<double*>(b1 + nl * pitch);
   const size_t N = size_t(n) * n * n;
   const size_t row0 = size_t(blockIdx.x) * rb;
-  const C* spec = reinterpret_cast<const C*>(A.spec) + size_t(load) * 3 * size_t(n) * n * ns;
+  const int nsp = A.nsp;
+  const C* spec = reinterpret_cast<const C*>(A.spec) + size_t(load) * 3 * size_t(n) * n * nsp;
   // Z[k] = A[k] + i B[k] over the full line, A/B Hermitian-extended; DC/Nyquist imaginary parts dropped
   const int total = nl * n;
   for (int i = tid; i < total; i += nthr) {
@@ -425,7 +474,7 @@ __global__ void __launch_bounds__(512) k_ifx(const GreenArgs A) {
     for (int h = 0; h < 2; ++h) {
       const int rho = 2 * l + h;
       const int rl = rho / 3, c = rho - 3 * rl;
-      const C* src = spec + (size_t(c) * n * n + row0 + rl) * ns;
+      const C* src = spec + (size_t(c) * n * n + row0 + rl) * nsp;
       C val;
       if (k < ns) {
         val = src[k];
@@ -442,7 +491,7 @@ __global__ void __launch_bounds__(512) k_ifx(const GreenArgs A) {
   }
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_lines<T>(b0, b1, threadIdx.x, pitch, A.plan, tw, true);
+  C* res = fft_line<T>(b0, b1, threadIdx.x * pitch, 1, A.plan, tw, true);
   T* sw = reinterpret_cast<T*>(A.sw) + size_t(load) * 3 * N;
   const double* sc = A.scale;
   double acc[3] = {0.0, 0.0, 0.0};
@@ -482,8 +531,8 @@ static size_t smem_x(const pgj_ctx* c, size_t cb) {
   const int nl = 3 * c->fg.rb / 2;
   return 2 * size_t(nl) * (c->n + 1) * cb + 32 * 3 * 8 + 64;
 }
-static size_t smem_y(const pgj_ctx* c, size_t cb) { return 2 * size_t(c->fg.kcy) * (c->n + 1) * cb; }
-static size_t smem_z(const pgj_ctx* c, size_t cb) { return 2 * 3 * size_t(c->fg.kcz) * (c->n + 1) * cb + 32 * 8 + 64; }
+static size_t smem_y(const pgj_ctx* c, size_t cb) { return 2 * size_t(c->fg.kcy) * c->n * cb + 16; }
+static size_t smem_z(const pgj_ctx* c, size_t cb) { return 2 * 3 * size_t(c->fg.kcz) * c->n * cb + 32 * 8 + 16; }
 
 template <typename T>
 static int set_smem_limits() {
@@ -528,11 +577,12 @@ static int run_green(pgj_ctx* c, int loads, GreenArgs& A, cudaStream_t s) {
 static GreenArgs green_args(pgj_ctx* c, int prec, const void* r) {
   GreenArgs A;
   std::memset(&A, 0, sizeof(A));
-  A.n = c->n; A.ns = c->ns; A.plan = c->plan; A.geo = c->fg;
+  A.n = c->n; A.ns = c->ns; A.nsp = c->ns + (c->ns & 1); A.plan = c->plan; A.geo = c->fg;
   A.r = r; A.scale = c->scale; A.spec = c->spec;
   A.sym = prec == PGJ_FP32 ? static_cast<const void*>(c->symbol32) : static_cast<const void*>(c->symbol);
   A.tw = prec == PGJ_FP32 ? static_cast<const void*>(static_cast<double2*>(c->tw) + c->n) : c->tw;
   A.sw = c->sw; A.scal = c->scal; A.partials = c->partials;
+  A.err = c->cond + 2;
   return A;
 }
 

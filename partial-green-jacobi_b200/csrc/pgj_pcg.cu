@@ -100,8 +100,18 @@ __global__ void __launch_bounds__(256) k_update_ur(int n, U* __restrict__ u, T* 
   }
 }
 
+// Blocks per load for the vector updates: about four 48-byte chunks per thread (enough loads in
+// flight per thread, few blocks paying the reduction), at least 16 and at most 296 per load.
+static unsigned update_blocks(const pgj_ctx* c, int prec) {
+  const size_t chunks = 3 * size_t(c->N) / (prec == PGJ_FP32 ? 12 : 6);
+  size_t b = (chunks + 256 * 4 - 1) / (256 * 4);
+  if (b < 16) b = 16;
+  if (b > 296) b = 296;
+  return unsigned(b);
+}
+
 int launch_update_ur(pgj_ctx* c, int loads, int prec, double* u64, void* uT, cudaStream_t s) {
-  dim3 grid(2 * 148, loads);
+  dim3 grid(update_blocks(c, prec), loads);
   const double rel = c->rel_delta2;
   if (prec == PGJ_FP32) {
     if (u64)
@@ -163,7 +173,7 @@ __global__ void __launch_bounds__(256) k_update_p(int n, int loads, T* __restric
 
 int launch_update_p(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, cudaGraphConditionalHandle h,
                     bool set_cond) {
-  dim3 grid(2 * 148, loads);
+  dim3 grid(update_blocks(c, prec), loads);
   if (prec == PGJ_FP32)
     k_update_p<float><<<grid, 256, 0, s>>>(c->n, loads, static_cast<float*>(c->p), static_cast<const float*>(c->sw),
                                            c->scal, init ? 1 : 0, h, set_cond ? 1 : 0, c->cond);

@@ -321,7 +321,7 @@ def test_profile_iteration_reports_all_kernels(pkg):
 def test_batch_concurrent_designs_match_single_solves(pkg, precision):
     """Designs of uneven n in flight on separate streams give the single-design results."""
     lam, mu = pkg.PAPER_MEDIUM
-    designs = [(12, 3, 1e-4, 0.5), (16, 4, 1e-6, 0.25), (12, 5, 1e-9, 1.0), (16, 6, 1e-6, 0.0), (16, 7, 1e-4, 0.75)]
+    designs = [(12, 3, 1e-4, 0.5), (16, 4, 1e-6, 0.25), (12, 5, 1e-9, 1.0), (16, 6, 1e-4, 0.0), (16, 7, 1e-4, 0.75)]
     reqs = [pkg.Request(torch.tensor(pkg.baseline_design(n, seed, emin)), alpha, tag=i)
             for i, (n, seed, emin, alpha) in enumerate(designs)]
     batch = pkg.Batch(slots=2, precision=precision)
@@ -358,3 +358,26 @@ def test_async_solve_equals_blocking_solve(pkg):
     assert L.pgj_solve_wait(op._ctx, info, s) == 0
     assert st1 == 0 and [i.iterations for i in info] == [i["iterations"] for i in infos1]
     assert torch.equal(u1, u2)
+
+
+def test_green_alpha0_fails_certification_like_the_oracle(pkg, oracle):
+    """alpha=0 (pure Green) at Emin=1e-6 does not certify within 4000 iterations (the reference records
+    141 such failures in data/study2/replay_parallel_summary.csv:7); the device path must report the
+    same failure instead of a result."""
+    n = 16
+    lam, mu = pkg.PAPER_MEDIUM
+    a = pkg.baseline_design(n, 6, 1e-6)
+    ref = oracle.homogenize(a, lam, mu, 0.0)
+    assert ref["raised"] and all(i.iterations == 4000 for i in ref["infos"])
+    op = pkg.Operator(n, 6, lam, mu)
+    op.set_material(dev(a))
+    op.set_alpha(0.0)
+    u = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")
+    infos, st = op.solve(np.eye(6), 1e-8, u)
+    assert st == pkg._lib.PGJ_ERR_CERTIFICATION
+    assert all(i["iterations"] == 4000 and not i["converged"] for i in infos)
+    r = pkg.PaperResident(None, n, "shear", 0.2, emin=1e-6)
+    r.material(dev(a))
+    r.select("green")
+    with pytest.raises(RuntimeError, match="true residual certification failed"):
+        r.solve()
