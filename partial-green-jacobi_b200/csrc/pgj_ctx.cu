@@ -416,6 +416,7 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
   if (!st) st = launch_scale(c, 0.5, s);  // stages the diagonal constants (once)
   if (!st) st = launch_scale(c, 0.0, s);  // scale = 1 until an alpha is selected
   if (!st) st = autotune_stencil(c, s);
+  if (!st) st = autotune_fft(c, s);
   if (st) {
     delete c->graphs;
     delete c;

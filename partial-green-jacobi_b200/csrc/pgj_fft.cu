@@ -16,6 +16,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 namespace pgj {
@@ -40,7 +43,7 @@ bool make_fft_plan(int n, FFTPlan* plan) {
 // smem budget per block for the line buffers (two ping-pong buffers)
 static constexpr size_t kFFTSmemBudget = 200 * 1024;
 
-FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan) {
+FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan, int rb_req, int nky_req, int nkz_req) {
   FFTGeom g;
   const size_t cb = 2 * size_t(elem_bytes);  // complex bytes
   const size_t line = size_t(n + 1) * cb;
@@ -60,7 +63,7 @@ FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan) {
     return v ? std::atoi(v) : dflt;
   };
   // x passes: rb rows (z,y) -> 3 rb / 2 complex lines, rb | n*n, at most ~48 lines
-  int rb = env("PGJ_FFT_RB", 16);
+  int rb = env("PGJ_FFT_RB", rb_req > 0 ? rb_req : 16);
   while (rb > 2 && ((size_t(n) * n) % rb != 0 || 2 * (3 * size_t(rb) / 2) * line > kFFTSmemBudget ||
                     3 * rb / 2 > 512))
     rb /= 2;
@@ -69,12 +72,12 @@ FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan) {
   const int nsp = ns + (ns & 1);
   auto even_up = [](int v) { return (v + 1) & ~1; };
   const size_t budget_y = 100 * 1024, budget_z = 120 * 1024;
-  int nky = env("PGJ_FFT_NKY", 1);
+  int nky = env("PGJ_FFT_NKY", nky_req > 0 ? nky_req : 1);
   while (nky < nsp && 2 * size_t(n) * even_up((nsp + nky - 1) / nky) * cb > budget_y) ++nky;
   g.nky = nky;
   g.kcy = even_up((nsp + nky - 1) / nky);
   g.nky = (nsp + g.kcy - 1) / g.kcy;
-  int nkz = env("PGJ_FFT_NKZ", 1);
+  int nkz = env("PGJ_FFT_NKZ", nkz_req > 0 ? nkz_req : 1);
   while (nkz < nsp && (2 * 3 * size_t(n) * even_up((nsp + nkz - 1) / nkz) * cb > budget_z ||
                        3 * even_up((nsp + nkz - 1) / nkz) > 512))
     ++nkz;
@@ -317,9 +320,12 @@ __device__ __forceinline__ bool tile_load(C* dst, int rows, int kcp, unsigned by
   }
   __syncthreads();
   if (tid < 32) {
+    // lanes of warp 0 that exist (blocks of small grids have fewer than 32 threads)
+    const int lanes = min(32, block_threads());
+    const unsigned mask = lanes == 32 ? 0xffffffffu : ((1u << lanes) - 1u);
     if (tid == 0) mbar_expect_tx(bar, bytes * unsigned(rows));
-    __syncwarp();
-    for (int r = tid; r < rows; r += 32) tma_row(dst + size_t(r) * kcp, addr(r), bytes, bar);
+    __syncwarp(mask);
+    for (int r = tid; r < rows; r += lanes) tma_row(dst + size_t(r) * kcp, addr(r), bytes, bar);
   }
   const bool ok = mbar_wait(bar, 0);
   if (__syncthreads_or(!ok)) {
@@ -335,7 +341,8 @@ __device__ __forceinline__ void tile_store(const C* src, int rows, int kcp, unsi
   fence_proxy_async();
   __syncthreads();
   if (tid < 32) {
-    for (int r = tid; r < rows; r += 32) tma_store_row(addr(r), src + size_t(r) * kcp, bytes);
+    const int lanes = min(32, block_threads());
+    for (int r = tid; r < rows; r += lanes) tma_store_row(addr(r), src + size_t(r) * kcp, bytes);
     tma_store_commit();
     tma_store_wait_read();
   }
@@ -624,6 +631,61 @@ int launch_green_standalone(pgj_ctx* c, int loads, const double* r, double* z, c
   A.finalize_fz = 0;
   if ((st = run_green<double>(c, loads, A, s))) return st;
   k_project_out<<<dim3(296, loads), 256, 0, s>>>(c->n, static_cast<const double*>(c->sw), z, c->scal);
+  return check_launch();
+}
+
+// Green-apply autotuner: times the five passes (all loads active) for candidate tile shapes
+// (rows per x block, y-chunks, z-chunks) on the context's buffers; cached per (n, loads, precision).
+static std::mutex g_fft_mutex;
+static std::map<std::tuple<int, int, int>, FFTGeom> g_fft_tuned;
+
+int autotune_fft(pgj_ctx* c, cudaStream_t s) {
+  const auto key = std::make_tuple(c->n, c->L, c->prec);
+  {
+    std::lock_guard<std::mutex> lock(g_fft_mutex);
+    auto it = g_fft_tuned.find(key);
+    if (it != g_fft_tuned.end()) { c->fg = it->second; return PGJ_OK; }
+  }
+  if (std::getenv("PGJ_FFT_RB") || std::getenv("PGJ_FFT_NKY") || std::getenv("PGJ_FFT_NKZ")) return PGJ_OK;
+  const int eb = c->prec == PGJ_FP32 ? 4 : 8;
+  std::vector<FFTGeom> cands;
+  for (int rb : {8, 16})
+    for (int nky : {1, 2, 3})
+      for (int nkz : {1, 2, 3, 4, 6}) {
+        FFTGeom g = fft_geom(c->n, eb, c->plan, rb, nky, nkz);
+        bool dup = false;
+        for (const FFTGeom& h : cands)
+          dup = dup || (h.rb == g.rb && h.kcy == g.kcy && h.kcz == g.kcz);
+        if (!dup) cands.push_back(g);
+      }
+  GreenArgs A = green_args(c, c->prec, c->r);
+  A.skip_inactive = 0;
+  A.use_mean = 0;
+  A.finalize_fz = 0;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  FFTGeom best = c->fg;
+  float best_ms = 1e30f;
+  for (const FFTGeom& g : cands) {
+    c->fg = g;
+    A.geo = g;
+    int st = c->prec == PGJ_FP32 ? run_green<float>(c, c->L, A, s) : run_green<double>(c, c->L, A, s);
+    if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); c->fg = best; return st; }
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3; ++r)
+      c->prec == PGJ_FP32 ? run_green<float>(c, c->L, A, s) : run_green<double>(c, c->L, A, s);
+    cudaEventRecord(e1, s);
+    cudaEventSynchronize(e1);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (ms < best_ms) { best_ms = ms; best = g; }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->fg = best;
+  std::lock_guard<std::mutex> lock(g_fft_mutex);
+  g_fft_tuned[key] = best;
   return check_launch();
 }
 

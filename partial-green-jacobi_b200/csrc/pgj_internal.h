@@ -37,7 +37,7 @@ struct FFTGeom {
   int by_x, by_y, by_z;     // threads along y (butterflies of a line) per pass; x (and z) index lines
   FastDiv div_3n, div_ns, div_n, div_kcz;
 };
-FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan);
+FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan, int rb_req = 0, int nky_req = 0, int nkz_req = 0);
 
 enum StencilMode { kPlain = 0, kPCG = 1, kResidual = 2 };
 
@@ -165,6 +165,8 @@ int set_cuda_error(cudaError_t e);
 int prepare_stencil_kernels();
 // times candidate tile shapes of the operator on the context's buffers and keeps the fastest
 int autotune_stencil(pgj_ctx* c, cudaStream_t s);
+// times candidate tile shapes of the Green passes and keeps the fastest
+int autotune_fft(pgj_ctx* c, cudaStream_t s);
 int prepare_fft_kernels();
 inline int check_launch() {
   cudaError_t e = cudaGetLastError();
