@@ -152,8 +152,13 @@ def cpu_sample(n=N_GRID, seed=0, iters=4, its_full=None):
 
 
 # ------------------------------------------------------------------------------------------ GPU
+def design_seeds(rank, count=NSEEDS):
+    """Replicas only: every rank homogenizes its own designs (disjoint seeds), no data exchange."""
+    return [rank * 1000 + k for k in range(count)]
+
+
 def designs_for(rank, pkg):
-    return [pkg.baseline_design(N_GRID, rank * 1000 + k, EMIN) for k in range(NSEEDS)]
+    return [pkg.baseline_design(N_GRID, s, EMIN) for s in design_seeds(rank)]
 
 
 def run_gpu(args, rank, world, local_rank):

@@ -148,6 +148,12 @@ long long pgj_last_launches(pgj_ctx* ctx);
 int pgj_profile_iteration(pgj_ctx* ctx, int loads, const double* macros, int reps, double* ms, double* bytes,
                           void* stream);
 
+/* Failure-detection self-test (no reference counterpart): runs the bounded device wait used by the
+ * kernels' TMA staging on an mbarrier that nothing completes, giving up after `tries` polls.
+ * Returns PGJ_ERR_TIMEOUT when the wait expired and was reported (the expected outcome); the
+ * context stays usable. Never faults or hangs: no copy is issued and the wait is bounded. */
+int pgj_selftest_wait_timeout(pgj_ctx* ctx, int tries, void* stream);
+
 /* ------------------------------------------------------------------ responses
  * Per-element energies e_l = v^T Ke(C0) v / h^3, v = u_l + A_l (affine macro field), for each of
  * `loads` (u, macros); e: (loads, N) device (energy.cu evaluate,

@@ -48,8 +48,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
 }
 // Bounded wait: gives up after kMaxTries polls (each poll may suspend briefly in hardware).
 constexpr int kMaxTries = 1 << 20;
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  for (int i = 0; i < kMaxTries; ++i)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity, int max_tries = kMaxTries) {
+  for (int i = 0; i < max_tries; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

@@ -667,6 +667,20 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
 
 long long pgj_last_launches(pgj_ctx* c) { return c ? c->last_launches : -1; }
 
+int pgj_selftest_wait_timeout(pgj_ctx* c, int tries, void* stream) {
+  if (!c || tries < 1) return PGJ_ERR_ARGUMENT;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  cudaError_t e = cudaMemsetAsync(c->cond + 6, 0, sizeof(int), s);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  int st = launch_wait_selftest(tries, c->cond + 6, s);
+  if (st) return st;
+  int flag = 0;
+  e = cudaMemcpyAsync(&flag, c->cond + 6, sizeof(int), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) return set_cuda_error(e);
+  return flag ? PGJ_ERR_TIMEOUT : PGJ_OK;
+}
+
 int pgj_profile_iteration(pgj_ctx* c, int loads, const double* macros, int reps, double* ms, double* bytes,
                           void* stream) {
   if (!c || !macros || !ms || !bytes || loads < 1 || loads > c->L || reps < 1) return PGJ_ERR_ARGUMENT;

@@ -68,21 +68,16 @@ FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan, int rb_req, int nky
                     3 * rb / 2 > 512))
     rb /= 2;
   g.rb = rb;
-  // y and z passes: tiles of kx columns, an even count so every copied row is 16-byte aligned
-  const int nsp = ns + (ns & 1);
-  auto even_up = [](int v) { return (v + 1) & ~1; };
-  const size_t budget_y = 100 * 1024, budget_z = 120 * 1024;
+  // y and z passes: tiles of kx columns (lines with pitch n+1 in shared memory)
+  const size_t budget_y = 200 * 1024, budget_z = 200 * 1024;
   int nky = env("PGJ_FFT_NKY", nky_req > 0 ? nky_req : 1);
-  while (nky < nsp && 2 * size_t(n) * even_up((nsp + nky - 1) / nky) * cb > budget_y) ++nky;
-  g.nky = nky;
-  g.kcy = even_up((nsp + nky - 1) / nky);
-  g.nky = (nsp + g.kcy - 1) / g.kcy;
+  while (nky < ns && ((ns + nky - 1) / nky > 64 || 2 * size_t((ns + nky - 1) / nky) * line > budget_y)) ++nky;
+  g.kcy = (ns + nky - 1) / nky;
+  g.nky = (ns + g.kcy - 1) / g.kcy;
   int nkz = env("PGJ_FFT_NKZ", nkz_req > 0 ? nkz_req : 1);
-  while (nkz < nsp && (2 * 3 * size_t(n) * even_up((nsp + nkz - 1) / nkz) * cb > budget_z ||
-                       3 * even_up((nsp + nkz - 1) / nkz) > 512))
-    ++nkz;
-  g.kcz = even_up((nsp + nkz - 1) / nkz);
-  g.nkz = (nsp + g.kcz - 1) / g.kcz;
+  while (nkz < ns && (3 * ((ns + nkz - 1) / nkz) > 48 || 2 * 3 * size_t((ns + nkz - 1) / nkz) * line > budget_z)) ++nkz;
+  g.kcz = (ns + nkz - 1) / nkz;
+  g.nkz = (ns + g.kcz - 1) / g.kcz;
   g.by_x = by_for(3 * g.rb / 2);
   g.by_y = by_for(g.kcy);
   g.by_z = by_for(3 * g.kcz);
@@ -244,7 +239,6 @@ struct GreenArgs {
   int use_mean;          // subtract scal.mean_r before scaling (projection P of the input)
   int init;              // FZ finalizer: initialise rz instead of forming beta
   int finalize_fz;       // FZ last block forms rz / beta (recurrence use only)
-  int* err;              // set to 1 if a bounded device wait expired
 };
 
 __device__ __forceinline__ bool load_on(const GreenArgs& A, int load) {
@@ -306,50 +300,8 @@ __global__ void __launch_bounds__(512) k_fx(const GreenArgs A) {
   }
 }
 
-// ---------------------------------------------------------------------------- row-tile staging
-// A block's tile is a set of spectrum rows, each `bytes` long and 16-byte aligned, copied with TMA
-// bulk copies into shared memory in their natural layout (row r at r * kcp). One elected warp issues
-// the copies; the block waits on an mbarrier with a bounded poll (timeout -> error flag, early exit).
-template <typename C, typename RowAddr>
-__device__ __forceinline__ bool tile_load(C* dst, int rows, int kcp, unsigned bytes, RowAddr addr, uint64_t* bar,
-                                          int* err) {
-  const int tid = flat_tid();
-  if (tid == 0) {
-    mbar_init(bar, 1);
-    fence_mbar_init();
-  }
-  __syncthreads();
-  if (tid < 32) {
-    // lanes of warp 0 that exist (blocks of small grids have fewer than 32 threads)
-    const int lanes = min(32, block_threads());
-    const unsigned mask = lanes == 32 ? 0xffffffffu : ((1u << lanes) - 1u);
-    if (tid == 0) mbar_expect_tx(bar, bytes * unsigned(rows));
-    __syncwarp(mask);
-    for (int r = tid; r < rows; r += lanes) tma_row(dst + size_t(r) * kcp, addr(r), bytes, bar);
-  }
-  const bool ok = mbar_wait(bar, 0);
-  if (__syncthreads_or(!ok)) {
-    if (tid == 0 && err) atomicExch(err, 1);
-    return false;
-  }
-  return true;
-}
-
-template <typename C, typename RowAddr>
-__device__ __forceinline__ void tile_store(const C* src, int rows, int kcp, unsigned bytes, RowAddr addr) {
-  const int tid = flat_tid();
-  fence_proxy_async();
-  __syncthreads();
-  if (tid < 32) {
-    const int lanes = min(32, block_threads());
-    for (int r = tid; r < rows; r += lanes) tma_store_row(addr(r), src + size_t(r) * kcp, bytes);
-    tma_store_commit();
-    tma_store_wait_read();
-  }
-}
-
 // ---------------------------------------------------------------------------- FY / IFY
-// block (kcy lines, by): one (load, component, z) plane, kx columns k0..k0+kcy of every y row.
+// block (kcy lines, by): one (load, component, z) plane, kx columns k0..k0+kcy.
 template <typename T, bool INV>
 __global__ void __launch_bounds__(512) k_fy(const GreenArgs A) {
   using C = cplx<T>;
@@ -357,54 +309,49 @@ __global__ void __launch_bounds__(512) k_fy(const GreenArgs A) {
   const int lc = blockIdx.z;  // load * 3 + component
   const int load = lc / 3, c = lc - 3 * load;
   if (!load_on(A, load)) return;
-  const int n = A.n, ns = A.ns, nsp = A.nsp, kc = A.geo.kcy;
+  const int n = A.n, ns = A.ns, nsp = A.nsp, pitch = n + 1, kc = A.geo.kcy;
   const int z = blockIdx.y;
   const int k0 = blockIdx.x * kc;
-  const int kn = min(kc, ns - k0);    // live columns
-  const int kcp = min(kc, nsp - k0);  // columns copied (even: 16-byte rows)
+  const int kn = min(kc, ns - k0);
   const int kl = threadIdx.x;
   C* b0 = reinterpret_cast<C*>(smem_raw);
-  C* b1 = b0 + size_t(n) * kc;
-  uint64_t* bar = reinterpret_cast<uint64_t*>(b1 + size_t(n) * kc);
-  C* plane = reinterpret_cast<C*>(A.spec) + (size_t(load) * 3 + c) * size_t(n) * n * nsp + size_t(z) * n * nsp + k0;
-  const unsigned bytes = unsigned(kcp * sizeof(C));
-  if (!tile_load(b0, n, kcp, bytes, [&](int y) { return plane + size_t(y) * nsp; }, bar, A.err)) return;
+  C* b1 = b0 + kc * pitch;
+  C* plane = reinterpret_cast<C*>(A.spec) + (size_t(load) * 3 + c) * size_t(n) * n * nsp + size_t(z) * n * nsp;
+  if (kl < kn)
+    for (int y = threadIdx.y; y < n; y += blockDim.y) b0[kl * pitch + y] = plane[size_t(y) * nsp + k0 + kl];
+  __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_line<T>(b0, b1, kl < kn ? kl : -1, kcp, A.plan, tw, INV);
-  tile_store(res, n, kcp, bytes, [&](int y) { return plane + size_t(y) * nsp; });
+  C* res = fft_line<T>(b0, b1, kl < kn ? kl * pitch : -1, 1, A.plan, tw, INV);
+  if (kl < kn)
+    for (int y = threadIdx.y; y < n; y += blockDim.y) plane[size_t(y) * nsp + k0 + kl] = res[kl * pitch + y];
 }
 
 // ---------------------------------------------------------------------------- FZ (+ symbol)
-// block (kcz, by, 3): one (load, ky), kx columns k0..k0+kcz, the three components along z; rows
-// (c, z) of the tile at (c n + z) * kcp.
+// block (kcz, by, 3): one (load, ky), kx columns k0..k0+kcz, the three components along z.
 template <typename T>
 __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int load = blockIdx.z;
   if (!load_on(A, load)) return;
-  const int n = A.n, ns = A.ns, nsp = A.nsp, kc = A.geo.kcz;
+  const int n = A.n, ns = A.ns, nsp = A.nsp, pitch = n + 1, kc = A.geo.kcz;
   const int ky = blockIdx.y;
   const int k0 = blockIdx.x * kc;
   const int kn = min(kc, ns - k0);
-  const int kcp = min(kc, nsp - k0);
   const int kl = threadIdx.x, c = threadIdx.z;
   const int tid = flat_tid();
   C* b0 = reinterpret_cast<C*>(smem_raw);
-  C* b1 = b0 + size_t(3) * n * kc;
-  double* red = reinterpret_cast<double*>(b1 + size_t(3) * n * kc);
-  uint64_t* bar = reinterpret_cast<uint64_t*>(red + 32);
+  C* b1 = b0 + 3 * kc * pitch;
+  double* red = reinterpret_cast<double*>(b1 + 3 * kc * pitch);
   const size_t plane = size_t(n) * n * nsp;  // one component
-  C* sp = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * plane + size_t(ky) * nsp + k0;
-  const unsigned bytes = unsigned(kcp * sizeof(C));
-  auto row = [&](int r) {  // r = c * n + z
-    const int cc = r / n, zz = r - cc * n;
-    return sp + cc * plane + size_t(zz) * n * nsp;
-  };
-  if (!tile_load(b0, 3 * n, kcp, bytes, row, bar, A.err)) return;
-  const int off = kl < kn ? c * n * kcp + kl : -1;
+  C* sp = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * plane;
+  const int line = c * kc + kl;
+  if (kl < kn)
+    for (int z = threadIdx.y; z < n; z += blockDim.y)
+      b0[line * pitch + z] = sp[c * plane + (size_t(z) * n + ky) * nsp + k0 + kl];
+  __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_line<T>(b0, b1, off, kcp, A.plan, tw, false);
+  C* res = fft_line<T>(b0, b1, kl < kn ? line * pitch : -1, 1, A.plan, tw, false);
   // symbol multiply and Parseval partial sum: rows kz over (threadIdx.y, threadIdx.z)
   const T* sym = reinterpret_cast<const T*>(A.sym);
   const size_t Nh = size_t(n) * n * ns;
@@ -416,9 +363,9 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
       const size_t kk = (size_t(kz) * n + ky) * ns + kx;
       const T c0 = sym[kk], c1 = sym[Nh + kk], c2 = sym[2 * Nh + kk];
       const T c3 = sym[3 * Nh + kk], c4 = sym[4 * Nh + kk], c5 = sym[5 * Nh + kk];
-      C* px = res + (0 * n + kz) * kcp + kl;
-      C* py = res + (1 * n + kz) * kcp + kl;
-      C* pz = res + (2 * n + kz) * kcp + kl;
+      C* px = res + (0 * kc + kl) * pitch + kz;
+      C* py = res + (1 * kc + kl) * pitch + kz;
+      C* pz = res + (2 * kc + kl) * pitch + kz;
       const C x = *px, y = *py, zv = *pz;
       C wx, wy, wz;
       wx.x = c0 * x.x + c3 * y.x + c4 * zv.x; wx.y = c0 * x.y + c3 * y.y + c4 * zv.y;
@@ -431,8 +378,10 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
   }
   __syncthreads();
   C* other = (res == b0) ? b1 : b0;
-  C* res2 = fft_line<T>(res, other, off, kcp, A.plan, tw, true);
-  tile_store(res2, 3 * n, kcp, bytes, row);
+  C* res2 = fft_line<T>(res, other, kl < kn ? line * pitch : -1, 1, A.plan, tw, true);
+  if (kl < kn)
+    for (int z = threadIdx.y; z < n; z += blockDim.y)
+      sp[c * plane + (size_t(z) * n + ky) * nsp + k0 + kl] = res2[line * pitch + z];
   if (!A.finalize_fz) return;
   block_sum<1>(acc, red);
   const int nblk = gridDim.x * gridDim.y, blk = blockIdx.x + gridDim.x * blockIdx.y;
@@ -538,8 +487,8 @@ static size_t smem_x(const pgj_ctx* c, size_t cb) {
   const int nl = 3 * c->fg.rb / 2;
   return 2 * size_t(nl) * (c->n + 1) * cb + 32 * 3 * 8 + 64;
 }
-static size_t smem_y(const pgj_ctx* c, size_t cb) { return 2 * size_t(c->fg.kcy) * c->n * cb + 16; }
-static size_t smem_z(const pgj_ctx* c, size_t cb) { return 2 * 3 * size_t(c->fg.kcz) * c->n * cb + 32 * 8 + 16; }
+static size_t smem_y(const pgj_ctx* c, size_t cb) { return 2 * size_t(c->fg.kcy) * (c->n + 1) * cb; }
+static size_t smem_z(const pgj_ctx* c, size_t cb) { return 2 * 3 * size_t(c->fg.kcz) * (c->n + 1) * cb + 32 * 8 + 64; }
 
 template <typename T>
 static int set_smem_limits() {
@@ -589,7 +538,6 @@ static GreenArgs green_args(pgj_ctx* c, int prec, const void* r) {
   A.sym = prec == PGJ_FP32 ? static_cast<const void*>(c->symbol32) : static_cast<const void*>(c->symbol);
   A.tw = prec == PGJ_FP32 ? static_cast<const void*>(static_cast<double2*>(c->tw) + c->n) : c->tw;
   A.sw = c->sw; A.scal = c->scal; A.partials = c->partials;
-  A.err = c->cond + 2;
   return A;
 }
 

@@ -163,6 +163,7 @@ int launch_effective_tensor(pgj_ctx* c, const double* u, double* C, double* e, c
 int set_cuda_error(cudaError_t e);
 // one-time kernel attributes (dynamic shared memory limits); called at context creation
 int prepare_stencil_kernels();
+int launch_wait_selftest(int tries, int* flag, cudaStream_t s);
 // times candidate tile shapes of the operator on the context's buffers and keeps the fastest
 int autotune_stencil(pgj_ctx* c, cudaStream_t s);
 // times candidate tile shapes of the Green passes and keeps the fastest

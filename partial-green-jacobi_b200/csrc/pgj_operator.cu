@@ -375,6 +375,25 @@ int autotune_stencil(pgj_ctx* c, cudaStream_t s) {
   return check_launch();
 }
 
+// Self-test of the bounded device wait: an mbarrier armed for 16 bytes that no copy will deliver;
+// the wait must give up after `tries` polls and report it. No asynchronous copy is ever issued.
+__global__ void k_wait_selftest(int tries, int* flag) {
+  __shared__ __align__(8) uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) mbar_expect_tx(&bar, 16);  // the transaction count never drains
+  const bool ok = mbar_wait(&bar, 0, tries);
+  if (__syncthreads_or(!ok) && threadIdx.x == 0) *flag = 1;
+}
+
+int launch_wait_selftest(int tries, int* flag, cudaStream_t s) {
+  k_wait_selftest<<<1, 32, 0, s>>>(tries, flag);
+  return check_launch();
+}
+
 int prepare_stencil_kernels() {
   const int lim = 220 * 1024;  // below the 227 KB opt-in less the static shared memory
   cudaFuncSetAttribute(k_stencil<float, kPlain>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);

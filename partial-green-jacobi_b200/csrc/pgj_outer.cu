@@ -63,11 +63,11 @@ __global__ void k_paper_sens_in(size_t N, const double* __restrict__ ph, const d
   }
 }
 
-// ratio = -(g / N) / dv, stored in place of g
+// ratio = -(g / N) / dv, stored in place of g (reproduction.py:92-95)
 __global__ void k_paper_ratio(size_t N, double* __restrict__ g, const double* __restrict__ dv, double* bounds) {
-  const double invN = 1.0 / double(N);
+  const double dN = double(N);
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x)
-    g[i] = -(g[i] * invN) / dv[i];
+    g[i] = -(g[i] / dN) / dv[i];
   if (blockIdx.x == 0 && threadIdx.x == 0) { bounds[0] = 0.0; bounds[1] = 1e9; bounds[2] = 1.0; bounds[3] = 0.0; }
 }
 

@@ -381,3 +381,60 @@ def test_green_alpha0_fails_certification_like_the_oracle(pkg, oracle):
     r.select("green")
     with pytest.raises(RuntimeError, match="true residual certification failed"):
         r.solve()
+
+
+# ------------------------------------------------------------------------------ design updates (OC)
+def test_study1_chain_matches_reference_fixture(pkg, golden_dir):
+    """Study I Gaussian filter, projection and 45-step OC vs the reference study.py functions (n=8)."""
+    d = np.load(golden_dir / "reference_cpu.npz")
+    n = 8
+    out = pkg.ResidentOuter(n)
+    out.set_initial(d["s1_x"])
+    out.evaluate(2.0)
+    assert rel(out.ph.cpu().numpy(), d["s1_ph"]) < 1e-13
+    assert rel(out.dp.cpu().numpy(), d["s1_dp"]) < 1e-13
+    out.step(torch.tensor(d["s1_energy"], device="cuda"))
+    # 45 fixed bisections can take an adjacent final branch (check_outer.py:38-40): 2e-8
+    assert rel(out.new.cpu().numpy(), d["s1_new"]) < 2e-8
+
+
+def test_paper_chain_matches_oracle(pkg, oracle):
+    """Study II clipped cone filter, tanh(beta,eta) projection and damped OC with the MATLAB stop."""
+    n, rmin, volume = 10, 2.1, 0.3
+    rng = np.random.default_rng(51)
+    x = rng.uniform(0.15, 0.7, (n, n, n))
+    energy = -rng.uniform(0.5, 1.5, (n, n, n))
+    po = pkg.PaperOuter(n, volume, rmin=rmin, beta=4.0, eta=0.5, emin=1e-9)
+    po.set_initial(x)
+    po.evaluate()
+    hs = oracle.cone_filter(np.ones((n, n, n)), rmin)
+    assert rel(po.hs.cpu().numpy(), hs) < 1e-13
+    ph, dp, a = oracle.paper_physical(oracle.cone_filter(x, rmin), hs)
+    assert rel(po.ph.cpu().numpy(), ph) < 1e-13 and rel(po.a.cpu().numpy(), a) < 1e-13
+    po.step(torch.tensor(energy, device="cuda"))
+    new, steps, change = oracle.paper_oc(x, energy, ph, dp, hs, rmin, volume)
+    assert po.steps == steps
+    assert rel(po.new.cpu().numpy(), new) < 1e-9
+    assert abs(po.change - change) < 1e-12
+
+
+def test_design_step_objective_and_sensitivity(pkg, oracle):
+    """One Study II design step: solve, shear objective / local energy, OC update (verify.py:39-96)."""
+    n = 8
+    lam, mu = pkg.PAPER_MEDIUM
+    r = pkg.PaperResident(None, n, "shear", 0.2, rmin=2.1)
+    rng = np.random.default_rng(3)
+    x = rng.uniform(0.15, 0.7, (n, n, n))
+    r.outer.set_initial(x)
+    r.outer.evaluate()
+    r.material(r.outer.a)
+    r.select("0.5")
+    r.solve(1e-11)
+    f, local, diag = r.energy(7)
+    a = r.outer.a.cpu().numpy()
+    out = oracle.homogenize(a, lam, mu, 0.5, rtol=1e-11)
+    e = oracle.energies(out["u"], oracle.affine(n, np.eye(6)), n, lam, mu)
+    local_ref = -e[3:].sum(0)
+    assert rel(local.cpu().numpy().ravel(), local_ref) < 1e-8
+    assert abs(float(f) - (local_ref * a.ravel()).mean()) < 1e-11
+    assert rel(diag.cpu().numpy(), (e * a.reshape(1, -1)).mean(1)) < 1e-8
