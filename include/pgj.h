@@ -148,6 +148,14 @@ long long pgj_last_launches(pgj_ctx* ctx);
 int pgj_profile_iteration(pgj_ctx* ctx, int loads, const double* macros, int reps, double* ms, double* bytes,
                           void* stream);
 
+/* Kernel set of the PCG iteration (no reference counterpart; both give the reference's recurrence).
+ * 1: four kernels per iteration (operator; update + x/y transforms; z pass; inverse x/y + direction
+ * update), used when a transform slab fits in shared memory; 0: the operator, the two vector updates
+ * and the five Green passes as separate kernels. pgj_set_fused_iteration returns
+ * PGJ_ERR_UNSUPPORTED for 1 when the slab does not fit. */
+int pgj_fused_iteration(pgj_ctx* ctx);
+int pgj_set_fused_iteration(pgj_ctx* ctx, int on);
+
 /* Failure-detection self-test (no reference counterpart): runs the bounded device wait used by the
  * kernels' TMA staging on an mbarrier that nothing completes, giving up after `tries` polls.
  * Returns PGJ_ERR_TIMEOUT when the wait expired and was reported (the expected outcome); the

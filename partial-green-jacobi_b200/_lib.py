@@ -66,6 +66,8 @@ SIGNATURES = {
     "pgj_last_refinements": (C.c_int, [vp]),
     "pgj_last_launches": (C.c_longlong, [vp]),
     "pgj_selftest_wait_timeout": (C.c_int, [vp, C.c_int, vp]),
+    "pgj_fused_iteration": (C.c_int, [vp]),
+    "pgj_set_fused_iteration": (C.c_int, [vp, C.c_int]),
     "pgj_profile_iteration": (C.c_int, [vp, C.c_int, vp, C.c_int, vp, vp, vp]),
     "pgj_energies": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),
     "pgj_effective_tensor": (C.c_int, [vp, vp, vp, vp]),

@@ -111,6 +111,28 @@ template <typename C> __device__ __forceinline__ C cmul_mi(C a, bool inv) {
 }
 template <typename C, typename T> __device__ __forceinline__ C cscale(C a, T s) { a.x *= s; a.y *= s; return a; }
 
+// --------------------------------------------------------------------------- batched copies
+// for (i = tid; i < count; i += nthr) st(i, ld(i)), with UNR loads issued before their stores so a
+// thread keeps UNR global reads in flight (a plain loop waits for each load before the next,
+// because the stores in between may alias the next load's address).
+template <int UNR, typename Ld, typename St>
+__device__ __forceinline__ void batched_copy(int tid, int nthr, int count, Ld ld, St st) {
+  using V = decltype(ld(0));
+  for (int i0 = tid; i0 < count; i0 += UNR * nthr) {
+    V v[UNR];
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+      const int i = i0 + u * nthr;
+      if (i < count) v[u] = ld(i);
+    }
+#pragma unroll
+    for (int u = 0; u < UNR; ++u) {
+      const int i = i0 + u * nthr;
+      if (i < count) st(i, v[u]);
+    }
+  }
+}
+
 // --------------------------------------------------------------------------- per-load solver scalars
 // One record per load, updated only by the last block of the kernel that owns the quantity.
 struct LoadScalars {

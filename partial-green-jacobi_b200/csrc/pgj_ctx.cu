@@ -9,6 +9,7 @@
 // certificate (the reference polls active.any() every 4 iterations).
 #include "pgj_internal.h"
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
@@ -71,6 +72,7 @@ static Layout make_layout(int n, int L, int prec) {
   y.q = take(tsz * N3 * L);
   y.sw = take(tsz * N3 * L);
   y.spec = take(2 * tsz * 3 * size_t(n) * n * nsp * L);
+  y.shat = take(2 * tsz * 3 * size_t(n) * n * nsp);
   y.total = o;
   return y;
 }
@@ -93,11 +95,31 @@ static int capture_iteration(pgj_ctx* c, int L, cudaStream_t s, cudaGraphConditi
   const int prec = c->prec;
   int st;
   if ((st = launch_stencil(c, kPCG, L, prec, c->p, c->q, nullptr, nullptr, s))) return st;
+  if (c->fused) {
+    // u += alpha p, r -= alpha q and the x/y transforms of s.r; z pass; inverse x/y and p update
+    if ((st = launch_fxy(c, L, prec, kSlabUpdateL, prec == PGJ_FP32 ? c->d : static_cast<void*>(c->x), s))) return st;
+    if ((st = launch_fz_fused(c, L, prec, false, s))) return st;
+    return launch_ifxy(c, L, prec, false, s, h, last);
+  }
   if (prec == PGJ_FP32) st = launch_update_ur(c, L, prec, nullptr, c->d, s);
   else st = launch_update_ur(c, L, prec, c->x, nullptr, s);
   if (st) return st;
   if ((st = launch_green(c, L, prec, c->r, false, s))) return st;
   return launch_update_p(c, L, prec, false, s, h, last);
+}
+
+// First direction p = M r of a recurrence (the masks are set): unfused Green + p = z, or the fused
+// form, which first refreshes DFT(s) in case the scale field was rewritten through its view.
+static int capture_first_direction(pgj_ctx* c, int L, cudaStream_t s) {
+  int st;
+  if (c->fused) {
+    if ((st = build_shat(c, s))) return st;
+    if ((st = launch_fxy(c, L, c->prec, kSlabInitL, nullptr, s))) return st;
+    if ((st = launch_fz_fused(c, L, c->prec, true, s))) return st;
+    return launch_ifxy(c, L, c->prec, true, s, 0, false);
+  }
+  st = launch_green(c, L, c->prec, c->r, true, s);
+  return st ? st : launch_update_p(c, L, c->prec, true, s, 0, false);
 }
 
 // Appends a conditional node of `type` after the current capture point of `s` and returns its body
@@ -155,8 +177,11 @@ static int capture_into(cudaGraph_t body, F&& fn) {
 // operator, update, IF(any load flagged){x += d; r64 = f - K64 x; r = T(r64)}, Green, p update.
 static int capture_iteration_rel(pgj_ctx* c, int L, cudaStream_t s, cudaGraphConditionalHandle hw) {
   int st;
+  const bool fused = c->fused != 0;
   if ((st = launch_stencil(c, kPCG, L, PGJ_FP32, c->p, c->q, nullptr, nullptr, s))) return st;
-  if ((st = launch_update_ur(c, L, PGJ_FP32, nullptr, c->d, s))) return st;
+  if (fused) st = launch_fxy(c, L, PGJ_FP32, kSlabUpdateL, c->d, s);
+  else st = launch_update_ur(c, L, PGJ_FP32, nullptr, c->d, s);
+  if (st) return st;
   cudaGraphConditionalHandle hif = 0;
   if ((st = make_handle(s, &hif, 0))) return st;
   if ((st = launch_rel_cond(c, L, hif, s))) return st;
@@ -170,9 +195,14 @@ static int capture_iteration_rel(pgj_ctx* c, int L, cudaStream_t s, cudaGraphCon
     r = launch_stencil(c, kResidual, L, PGJ_FP64, c->x, c->r64, c->f, nullptr, s3, c->scal_in);
     c->scal = saved;
     if (r) return r;
-    return launch_rel_sync(c, L, s3);
+    // flagged loads restart from T(r64); the fused form also re-transforms their residual
+    return fused ? launch_fxy(c, L, PGJ_FP32, kSlabSyncL, nullptr, s3) : launch_rel_sync(c, L, s3);
   });
   if (st) return st;
+  if (fused) {
+    if ((st = launch_fz_fused(c, L, PGJ_FP32, false, s))) return st;
+    return launch_ifxy(c, L, PGJ_FP32, false, s, hw, true);
+  }
   if ((st = launch_green(c, L, PGJ_FP32, c->r, false, s))) return st;
   return launch_update_p(c, L, PGJ_FP32, false, s, hw, true);
 }
@@ -186,8 +216,7 @@ static int end_capture(cudaStream_t s, cudaGraph_t* g, int st) {
 
 // Appends to the capture on `s`: directions init, then WHILE(any load active){iteration}.
 static int capture_pcg(pgj_ctx* c, int L, cudaStream_t s, bool reliable = false) {
-  int st = launch_green(c, L, c->prec, c->r, true, s);
-  if (!st) st = launch_update_p(c, L, c->prec, true, s, 0, false);
+  int st = capture_first_direction(c, L, s);
   if (st) return st;
   cudaStreamCaptureStatus cs;
   cudaGraph_t cg = nullptr;
@@ -383,6 +412,7 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
   c->x = reinterpret_cast<double*>(b + y.x);
   c->r64 = precision == PGJ_FP32 ? reinterpret_cast<double*>(b + y.r64) : nullptr;
   c->r = b + y.r; c->p = b + y.p; c->q = b + y.q; c->sw = b + y.sw; c->spec = b + y.spec;
+  c->shat = b + y.shat;
   c->partials = reinterpret_cast<double*>(b + y.partials);
   c->scal_out = reinterpret_cast<LoadScalars*>(b + y.scal);
   c->scal_in = c->scal_out + loads;
@@ -403,6 +433,8 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
   if (e != cudaSuccess) st = set_cuda_error(e);
   if (!st) st = prepare_stencil_kernels();
   if (!st) st = prepare_fft_kernels();
+  if (!st) st = prepare_slab_kernels();
+  c->fused = slab_fits(c) && !std::getenv("PGJ_UNFUSED") ? 1 : 0;
   if (!st) st = init_fft_tables(c, s);
   if (!st) st = build_symbol(n, lam, mu, c->symbol, c->symbol32, s);
   if (!st) {
@@ -558,10 +590,13 @@ int pgj_solve_wait(pgj_ctx* c, pgj_load_info* info, void* stream) {
     all = all && ok;
   }
   const long long attempts = cnt[4] + 1;
-  if (c->prec == PGJ_FP32)  // rel start, Green, p init, fold, certify, decide; 9 per body; 3 per replacement
-    c->last_launches = 2 + 3 + attempts * (7 + 1 + 3 + 1) + 9LL * cnt[5] + 3LL * cnt[3];
-  else  // init mask, Green, p init, certify, decide; 8 per body
-    c->last_launches = 2 + 3 + attempts * (7 + 3 + 1) + 8LL * cnt[5];
+  // loop body: operator, update, 5 Green passes, p update (fused: operator, fxy, fz, ifxy), plus the
+  // IF-condition kernel of the reliable-update form; the first direction is 7 kernels either way
+  const long long body = (c->fused ? 4 : 8) + (c->prec == PGJ_FP32 ? 1 : 0);
+  if (c->prec == PGJ_FP32)  // rel start, first direction, fold, certify, decide; 3 per replacement
+    c->last_launches = 2 + 3 + attempts * (7 + 1 + 3 + 1) + body * cnt[5] + 3LL * cnt[3];
+  else  // init mask, first direction, certify, decide
+    c->last_launches = 2 + 3 + attempts * (7 + 3 + 1) + body * cnt[5];
   c->last_refinements = c->prec == PGJ_FP32 ? 1 + cnt[3] : 1;
   if (cnt[2]) return PGJ_ERR_TIMEOUT;
   if (cnt[1]) return PGJ_ERR_ITERATION_CAP;
@@ -621,18 +656,18 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
       if ((e = cudaGraphLaunch(c->graphs->attempt, s)) != cudaSuccess) return set_cuda_error(e);
       ++sweeps;
       if ((e = read_state(true)) != cudaSuccess) return set_cuda_error(e);
-      // sweep: inner start + 5 Green passes + p init, 8 kernels per loop body, x += d, 3 certification kernels
-      launches += 1 + 6 + 8LL * body[0] + 1 + 3;
+      // sweep: inner start + first direction (6), loop bodies, x += d, 3 certification kernels
+      launches += 1 + 6 + (c->fused ? 4LL : 8LL) * body[0] + 1 + 3;
       if (body[1]) { capped_by_bound = true; break; }
     }
   } else {
     for (;;) {
       if ((e = cudaGraphLaunch(c->graphs->attempt, s)) != cudaSuccess) return set_cuda_error(e);
       if ((e = read_state(true)) != cudaSuccess) return set_cuda_error(e);
-      if (c->prec == PGJ_FP32)  // rel start + Green + p init, 9 per body, 3 per replacement, fold + certify
-        launches += 7 + 9LL * body[0] + 3LL * body[3] + 1 + 3;
-      else  // attempt: init mask + 5 Green passes + p init, 8 kernels per loop body, 3 certification kernels
-        launches += 7 + 8LL * body[0] + 3;
+      if (c->prec == PGJ_FP32)  // rel start + first direction, bodies, 3 per replacement, fold + certify
+        launches += 7 + (c->fused ? 5LL : 9LL) * body[0] + 3LL * body[3] + 1 + 3;
+      else  // attempt: init mask + first direction, loop bodies, 3 certification kernels
+        launches += 7 + (c->fused ? 4LL : 8LL) * body[0] + 3;
       if (body[1]) { capped_by_bound = true; break; }
       bool all, anybad, capped;
       evaluate(all, anybad, capped);
@@ -666,6 +701,17 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
 }
 
 long long pgj_last_launches(pgj_ctx* c) { return c ? c->last_launches : -1; }
+
+int pgj_fused_iteration(pgj_ctx* c) { return c ? c->fused : -1; }
+
+int pgj_set_fused_iteration(pgj_ctx* c, int on) {
+  if (!c || (on != 0 && on != 1)) return PGJ_ERR_ARGUMENT;
+  if (on && !slab_fits(c)) return PGJ_ERR_UNSUPPORTED;
+  c->fused = on;
+  c->graphs->loads = 0;  // rebuild the solve graphs with the other kernel set
+  c->graphs->attempt_loads = 0;
+  return PGJ_OK;
+}
 
 int pgj_selftest_wait_timeout(pgj_ctx* c, int tries, void* stream) {
   if (!c || tries < 1) return PGJ_ERR_ARGUMENT;
@@ -701,8 +747,9 @@ int pgj_profile_iteration(pgj_ctx* c, int loads, const double* macros, int reps,
   } else if ((st = launch_init_mask(c, loads, s))) {
     return st;
   }
-  if (!st) st = launch_green(c, loads, prec, c->r, true, s);
-  if (!st) st = launch_update_p(c, loads, prec, true, s, 0, false);
+  if (!st) st = capture_first_direction(c, loads, s);
+  const bool fused = c->fused != 0;
+  void* u = prec == PGJ_FP32 ? c->d : static_cast<void*>(c->x);
   cudaEvent_t ev[2 * PGJ_PROFILE_KERNELS];
   for (int k = 0; k < 2 * PGJ_PROFILE_KERNELS; ++k) cudaEventCreate(&ev[k]);
   double acc[PGJ_PROFILE_KERNELS] = {0};
@@ -710,6 +757,10 @@ int pgj_profile_iteration(pgj_ctx* c, int loads, const double* macros, int reps,
     for (int k = 0; k < PGJ_PROFILE_KERNELS && !st; ++k) {
       cudaEventRecord(ev[2 * k], s);
       if (k == 0) st = launch_stencil(c, kPCG, loads, prec, c->p, c->q, nullptr, nullptr, s);
+      else if (fused && k == 1) st = launch_fxy(c, loads, prec, kSlabUpdateL, u, s);
+      else if (fused && k == 2) st = launch_fz_fused(c, loads, prec, false, s);
+      else if (fused && k == 3) st = launch_ifxy(c, loads, prec, false, s, 0, false);
+      else if (fused) st = PGJ_OK;
       else if (k == 1) st = prec == PGJ_FP32 ? launch_update_ur(c, loads, prec, nullptr, c->d, s)
                                              : launch_update_ur(c, loads, prec, c->x, nullptr, s);
       else if (k < 7) st = launch_green_pass(c, loads, prec, c->r, false, k - 2, s);
@@ -730,6 +781,12 @@ int pgj_profile_iteration(pgj_ctx* c, int loads, const double* macros, int reps,
   const double V = double(N3) * sz * loads;           // one DOF vector over all loads
   const double S = double(Nh) * 3 * 2 * sz * loads;  // one complex half spectrum over all loads
   const double sc = double(N3) * 8.0;                 // scale field (FP64)
+  const double ub = prec == PGJ_FP32 ? V : 2 * V;   // iterate: FP64 x or the inner-precision correction
+  const double fused_algo[PGJ_PROFILE_KERNELS] = {
+      2 * V + 8.0 * N,                            // operator: read p (+a), write q
+      4 * V + ub + sc + S,                        // fxy: read p q r (+u +s), write r (+u), write spectrum
+      2 * S + 6.0 * Nh * sz + S / loads,          // fz: spectrum in/out, symbol, DFT(s)
+      S + sc + 2 * V, 0, 0, 0, 0};                // ifxy: read spectrum (+s) and p, write p
   const double algo[PGJ_PROFILE_KERNELS] = {
       2 * V + 8.0 * N,                  // operator: read p (+a), write q
       6 * V,                            // update_ur: read u p r q, write u r
@@ -741,7 +798,7 @@ int pgj_profile_iteration(pgj_ctx* c, int loads, const double* macros, int reps,
       3 * V};                           // update_p: read s.w p, write p
   for (int k = 0; k < PGJ_PROFILE_KERNELS; ++k) {
     ms[k] = acc[k] / reps;
-    bytes[k] = algo[k];
+    bytes[k] = fused ? fused_algo[k] : algo[k];
   }
   return PGJ_OK;
 }

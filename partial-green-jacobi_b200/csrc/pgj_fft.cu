@@ -12,7 +12,7 @@
 //   IFY: inverse along y.
 //   IFX: C2R along x (two rows per complex FFT), s.w and its per-component sums (projection P).
 // Loads whose recurrence is inactive are skipped block-uniformly.
-#include "pgj_internal.h"
+#include "pgj_fft_engine.cuh"
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -35,6 +35,7 @@ bool make_fft_plan(int n, FFTPlan* plan) {
   int ns = 1;
   for (int i = 0; i < plan->nst; ++i) {
     plan->ns_div[i] = make_fastdiv(unsigned(ns));
+    plan->nb_div[i] = make_fastdiv(unsigned(n / plan->radix[i]));
     ns *= plan->radix[i];
   }
   return m == 1 && n % 2 == 0 && n >= 4;
@@ -91,138 +92,6 @@ FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan, int rb_req, int nky
   return g;
 }
 
-// ----------------------------------------------------------------------------- radix kernels
-// Forward transforms use e^{-2 pi i jk/R}; inverse ones the conjugate (unnormalised).
-template <typename C>
-__device__ __forceinline__ void dft2(C& a, C& b) { C t = a; a = cadd(t, b); b = csub(t, b); }
-
-template <typename C>
-__device__ __forceinline__ void dft4(C& v0, C& v1, C& v2, C& v3, bool inv) {
-  C a = cadd(v0, v2), b = csub(v0, v2), c = cadd(v1, v3), d = cmul_mi(csub(v1, v3), inv);
-  v0 = cadd(a, c); v2 = csub(a, c); v1 = cadd(b, d); v3 = csub(b, d);
-}
-
-template <typename T, int R> struct Radix;
-
-template <typename T> struct Radix<T, 2> {
-  using C = cplx<T>;
-  static __device__ __forceinline__ void run(C (&v)[2], bool) { dft2(v[0], v[1]); }
-};
-template <typename T> struct Radix<T, 4> {
-  using C = cplx<T>;
-  static __device__ __forceinline__ void run(C (&v)[4], bool inv) { dft4(v[0], v[1], v[2], v[3], inv); }
-};
-template <typename T> struct Radix<T, 8> {
-  using C = cplx<T>;
-  static __device__ __forceinline__ void run(C (&v)[8], bool inv) {
-    const T r2 = T(0.70710678118654752440);
-    C e0 = v[0], e1 = v[2], e2 = v[4], e3 = v[6];
-    C o0 = v[1], o1 = v[3], o2 = v[5], o3 = v[7];
-    dft4(e0, e1, e2, e3, inv);
-    dft4(o0, o1, o2, o3, inv);
-    // twiddles W8^k (forward (1-i)/sqrt2 ...), conjugated for the inverse
-    C t1, t2, t3;
-    if (!inv) {
-      t1.x = r2 * (o1.x + o1.y); t1.y = r2 * (o1.y - o1.x);
-      t2.x = o2.y; t2.y = -o2.x;
-      t3.x = r2 * (o3.y - o3.x); t3.y = -r2 * (o3.x + o3.y);
-    } else {
-      t1.x = r2 * (o1.x - o1.y); t1.y = r2 * (o1.x + o1.y);
-      t2.x = -o2.y; t2.y = o2.x;
-      t3.x = -r2 * (o3.x + o3.y); t3.y = r2 * (o3.x - o3.y);
-    }
-    v[0] = cadd(e0, o0); v[4] = csub(e0, o0);
-    v[1] = cadd(e1, t1); v[5] = csub(e1, t1);
-    v[2] = cadd(e2, t2); v[6] = csub(e2, t2);
-    v[3] = cadd(e3, t3); v[7] = csub(e3, t3);
-  }
-};
-template <typename T> struct Radix<T, 3> {
-  using C = cplx<T>;
-  static __device__ __forceinline__ void run(C (&v)[3], bool inv) {
-    const T s3 = T(0.86602540378443864676);
-    C s = cadd(v[1], v[2]), d = csub(v[1], v[2]);
-    C t; t.x = v[0].x - T(0.5) * s.x; t.y = v[0].y - T(0.5) * s.y;
-    v[0] = cadd(v[0], s);
-    C u = cmul_mi(d, inv); u.x *= s3; u.y *= s3;
-    v[1] = cadd(t, u); v[2] = csub(t, u);
-  }
-};
-template <typename T> struct Radix<T, 5> {
-  using C = cplx<T>;
-  static __device__ __forceinline__ void run(C (&v)[5], bool inv) {
-    const T c1 = T(0.30901699437494742410), c2 = T(-0.80901699437494742410);
-    const T s1 = T(0.95105651629515357212), s2 = T(0.58778525229247312917);
-    C s14 = cadd(v[1], v[4]), d14 = csub(v[1], v[4]), s23 = cadd(v[2], v[3]), d23 = csub(v[2], v[3]);
-    C a1, a2, b1, b2;
-    a1.x = v[0].x + c1 * s14.x + c2 * s23.x; a1.y = v[0].y + c1 * s14.y + c2 * s23.y;
-    a2.x = v[0].x + c2 * s14.x + c1 * s23.x; a2.y = v[0].y + c2 * s14.y + c1 * s23.y;
-    b1.x = s1 * d14.x + s2 * d23.x; b1.y = s1 * d14.y + s2 * d23.y;
-    b2.x = s2 * d14.x - s1 * d23.x; b2.y = s2 * d14.y - s1 * d23.y;
-    v[0] = cadd(v[0], cadd(s14, s23));
-    C ib1 = cmul_mi(b1, inv), ib2 = cmul_mi(b2, inv);
-    v[1] = cadd(a1, ib1); v[4] = csub(a1, ib1);
-    v[2] = cadd(a2, ib2); v[3] = csub(a2, ib2);
-  }
-};
-
-// One Stockham stage on the line owned by this thread (its elements at stride es from `src` / `dst`),
-// butterflies j along threadIdx.y: out[(j/Ns)Ns R + j%Ns + r Ns] = DFT_R over r of
-// in[j + r n/R] * W^{r (j%Ns)}, W = e^{-2 pi i/(Ns R)}.
-template <typename T, int R>
-__device__ __forceinline__ void stage(const cplx<T>* __restrict__ src, cplx<T>* __restrict__ dst, int es, int n,
-                                      int Ns, const FastDiv& nsd, const cplx<T>* __restrict__ tw, bool inv) {
-  using C = cplx<T>;
-  const int nb = n / R;
-  const int step = n / (Ns * R);
-  for (int j = threadIdx.y; j < nb; j += blockDim.y) {
-    const int jq = fdiv(j, nsd);
-    const int jm = j - jq * Ns;
-    C v[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) v[r] = src[(j + r * nb) * es];
-    if (jm) {
-#pragma unroll
-      for (int r = 1; r < R; ++r) {
-        C w = tw[r * jm * step];
-        if (inv) w.y = -w.y;
-        v[r] = cmul(v[r], w);
-      }
-    }
-    Radix<T, R>::run(v, inv);
-    const int base = jq * Ns * R + jm;
-#pragma unroll
-    for (int r = 0; r < R; ++r) dst[(base + r * Ns) * es] = v[r];
-  }
-}
-
-// All stages on the thread's line at offset `off` (elements at stride es) of the ping-pong buffers
-// b0/b1; off < 0 marks an idle thread (it still joins the barriers). Returns the result buffer.
-template <typename T>
-__device__ cplx<T>* fft_line(cplx<T>* b0, cplx<T>* b1, int off, int es, const FFTPlan& pl, const cplx<T>* tw,
-                             bool inv) {
-  cplx<T>* src = b0;
-  cplx<T>* dst = b1;
-  int Ns = 1;
-  for (int st = 0; st < pl.nst; ++st) {
-    const int R = pl.radix[st];
-    const FastDiv& nsd = pl.ns_div[st];
-    if (off >= 0) {
-      switch (R) {
-        case 8: stage<T, 8>(src + off, dst + off, es, pl.n, Ns, nsd, tw, inv); break;
-        case 4: stage<T, 4>(src + off, dst + off, es, pl.n, Ns, nsd, tw, inv); break;
-        case 2: stage<T, 2>(src + off, dst + off, es, pl.n, Ns, nsd, tw, inv); break;
-        case 3: stage<T, 3>(src + off, dst + off, es, pl.n, Ns, nsd, tw, inv); break;
-        default: stage<T, 5>(src + off, dst + off, es, pl.n, Ns, nsd, tw, inv); break;
-      }
-    }
-    __syncthreads();
-    cplx<T>* t = src; src = dst; dst = t;
-    Ns *= R;
-  }
-  return src;
-}
-
 struct GreenArgs {
   int n, ns, nsp;  // grid edge, half-spectrum length, padded (even) spectrum row length
   FFTPlan plan;
@@ -239,6 +108,12 @@ struct GreenArgs {
   int use_mean;          // subtract scal.mean_r before scaling (projection P of the input)
   int init;              // FZ finalizer: initialise rz instead of forming beta
   int finalize_fz;       // FZ last block forms rz / beta (recurrence use only)
+  // slab-fused recurrence (the x/y transforms run in the PCG update kernels): the spectrum holds
+  // DFT(s.r); FZ subtracts mean_r . shat (shat = DFT(s)) and forms mean(s.w) by Parseval
+  const void* shat;      // (3, n, n, nsp) complex T: DFT of each component of the scale field
+  int fused;
+  int forward_only;      // FZ: forward transform along z only (builds shat)
+  int unit_input;        // FX: transform s itself (r ignored; builds shat)
 };
 
 __device__ __forceinline__ bool load_on(const GreenArgs& A, int load) {
@@ -266,17 +141,19 @@ __global__ void __launch_bounds__(512) k_fx(const GreenArgs A) {
   if (A.use_mean) { m[0] = T(A.scal[load].mean_r[0]); m[1] = T(A.scal[load].mean_r[1]); m[2] = T(A.scal[load].mean_r[2]); }
   const int total = rb * 3 * n;
   const size_t gbase = row0 * n * 3;
-  for (int i = tid; i < total; i += nthr) {
+  batched_copy<4>(tid, nthr, total, [&](int i) {
+    const size_t g = gbase + i;
+    const int c = i % 3;
+    const T mc = c == 0 ? m[0] : (c == 1 ? m[1] : m[2]);
+    return A.unit_input ? T(sc[g]) : T(sc[g]) * (r[g] - mc);
+  }, [&](int i, T v) {
     const int rl = fdiv(i, A.geo.div_3n);
     const int rem = i - rl * 3 * n;
     const int x = rem / 3, c = rem - 3 * x;
-    const size_t g = gbase + i;
-    const T mc = c == 0 ? m[0] : (c == 1 ? m[1] : m[2]);
-    const T v = T(sc[g]) * (r[g] - mc);
     const int rho = 3 * rl + c;
     T* dst = reinterpret_cast<T*>(b0 + (rho >> 1) * pitch + x);
     dst[rho & 1] = v;
-  }
+  });
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
   C* res = fft_line<T>(b0, b1, threadIdx.x * pitch, 1, A.plan, tw, false);
@@ -318,7 +195,8 @@ __global__ void __launch_bounds__(512) k_fy(const GreenArgs A) {
   C* b1 = b0 + kc * pitch;
   C* plane = reinterpret_cast<C*>(A.spec) + (size_t(load) * 3 + c) * size_t(n) * n * nsp + size_t(z) * n * nsp;
   if (kl < kn)
-    for (int y = threadIdx.y; y < n; y += blockDim.y) b0[kl * pitch + y] = plane[size_t(y) * nsp + k0 + kl];
+    batched_copy<8>(threadIdx.y, blockDim.y, n, [&](int y) { return plane[size_t(y) * nsp + k0 + kl]; },
+                    [&](int y, C v) { b0[kl * pitch + y] = v; });
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
   C* res = fft_line<T>(b0, b1, kl < kn ? kl * pitch : -1, 1, A.plan, tw, INV);
@@ -342,23 +220,33 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
   const int tid = flat_tid();
   C* b0 = reinterpret_cast<C*>(smem_raw);
   C* b1 = b0 + 3 * kc * pitch;
-  double* red = reinterpret_cast<double*>(b1 + 3 * kc * pitch);
+  double* red = reinterpret_cast<double*>(b1 + 3 * kc * pitch);  // 32 x 4 doubles
   const size_t plane = size_t(n) * n * nsp;  // one component
   C* sp = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * plane;
   const int line = c * kc + kl;
   if (kl < kn)
-    for (int z = threadIdx.y; z < n; z += blockDim.y)
-      b0[line * pitch + z] = sp[c * plane + (size_t(z) * n + ky) * nsp + k0 + kl];
+    batched_copy<8>(threadIdx.y, blockDim.y, n,
+                    [&](int z) { return sp[c * plane + (size_t(z) * n + ky) * nsp + k0 + kl]; },
+                    [&](int z, C v) { b0[line * pitch + z] = v; });
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
   C* res = fft_line<T>(b0, b1, kl < kn ? line * pitch : -1, 1, A.plan, tw, false);
-  // symbol multiply and Parseval partial sum: rows kz over (threadIdx.y, threadIdx.z)
+  if (A.forward_only) {
+    if (kl < kn)
+      for (int z = threadIdx.y; z < n; z += blockDim.y)
+        sp[c * plane + (size_t(z) * n + ky) * nsp + k0 + kl] = res[line * pitch + z];
+    return;
+  }
+  // symbol multiply and Parseval partial sums: rows kz over (threadIdx.y, threadIdx.z)
   const T* sym = reinterpret_cast<const T*>(A.sym);
+  const C* sh = reinterpret_cast<const C*>(A.shat);
   const size_t Nh = size_t(n) * n * ns;
-  double acc[1] = {0.0};
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
   if (kl < kn) {
     const int kx = k0 + kl;
     const double wgt = (kx == 0 || kx == n / 2) ? 1.0 : 2.0;
+    T m[3] = {T(0), T(0), T(0)};
+    if (A.fused) { m[0] = T(A.scal[load].mean_r[0]); m[1] = T(A.scal[load].mean_r[1]); m[2] = T(A.scal[load].mean_r[2]); }
     for (int kz = threadIdx.y + blockDim.y * threadIdx.z; kz < n; kz += blockDim.y * blockDim.z) {
       const size_t kk = (size_t(kz) * n + ky) * ns + kx;
       const T c0 = sym[kk], c1 = sym[Nh + kk], c2 = sym[2 * Nh + kk];
@@ -366,13 +254,28 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
       C* px = res + (0 * kc + kl) * pitch + kz;
       C* py = res + (1 * kc + kl) * pitch + kz;
       C* pz = res + (2 * kc + kl) * pitch + kz;
-      const C x = *px, y = *py, zv = *pz;
+      C x = *px, y = *py, zv = *pz;
+      C s0, s1, s2;
+      if (A.fused) {
+        // DFT(s.(r - mean r)) = DFT(s.r) - mean r . DFT(s)
+        const size_t ks = (size_t(kz) * n + ky) * nsp + kx;
+        s0 = sh[ks]; s1 = sh[plane + ks]; s2 = sh[2 * plane + ks];
+        x.x -= m[0] * s0.x; x.y -= m[0] * s0.y;
+        y.x -= m[1] * s1.x; y.y -= m[1] * s1.y;
+        zv.x -= m[2] * s2.x; zv.y -= m[2] * s2.y;
+      }
       C wx, wy, wz;
       wx.x = c0 * x.x + c3 * y.x + c4 * zv.x; wx.y = c0 * x.y + c3 * y.y + c4 * zv.y;
       wy.x = c3 * x.x + c1 * y.x + c5 * zv.x; wy.y = c3 * x.y + c1 * y.y + c5 * zv.y;
       wz.x = c4 * x.x + c5 * y.x + c2 * zv.x; wz.y = c4 * x.y + c5 * y.y + c2 * zv.y;
       acc[0] += wgt * (double(x.x) * wx.x + double(x.y) * wx.y + double(y.x) * wy.x + double(y.y) * wy.y +
                        double(zv.x) * wz.x + double(zv.y) * wz.y);
+      if (A.fused) {
+        // sum_x s w = sum_k W conj(DFT(s)) (1/N is folded into the symbol)
+        acc[1] += wgt * (double(wx.x) * s0.x + double(wx.y) * s0.y);
+        acc[2] += wgt * (double(wy.x) * s1.x + double(wy.y) * s1.y);
+        acc[3] += wgt * (double(wz.x) * s2.x + double(wz.y) * s2.y);
+      }
       *px = wx; *py = wy; *pz = wz;
     }
   }
@@ -383,14 +286,24 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
     for (int z = threadIdx.y; z < n; z += blockDim.y)
       sp[c * plane + (size_t(z) * n + ky) * nsp + k0 + kl] = res2[line * pitch + z];
   if (!A.finalize_fz) return;
-  block_sum<1>(acc, red);
   const int nblk = gridDim.x * gridDim.y, blk = blockIdx.x + gridDim.x * blockIdx.y;
   double* part = A.partials + size_t(load) * kPartialQ * kMaxPartials;
-  if (tid == 0) part[blk] = acc[0];
+  if (A.fused) {
+    block_sum<4>(acc, red);
+    if (tid == 0)
+      for (int k = 0; k < 4; ++k) part[k * kMaxPartials + blk] = acc[k];
+  } else {
+    double a1[1] = {acc[0]};
+    block_sum<1>(a1, red);
+    if (tid == 0) part[blk] = a1[0];
+  }
   LoadScalars& S = A.scal[load];
   if (!last_block(&S.ticket[kTicketFZ], nblk)) return;
   if (tid < 32) {
     const double rzn = warp_sum_partials(part, nblk);
+    double mz[3] = {0.0, 0.0, 0.0};
+    if (A.fused)
+      for (int k = 0; k < 3; ++k) mz[k] = warp_sum_partials(part + (k + 1) * kMaxPartials, nblk);
     if (tid == 0) {
       if (A.init) {
         S.beta = 0.0;
@@ -399,6 +312,8 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
         S.beta = rzn / (rz != 0.0 ? rz : 1.0);
       }
       S.rz = rzn;
+      if (A.fused)
+        for (int k = 0; k < 3; ++k) S.mean_z[k] = mz[k] / double(size_t(n) * n * n);
     }
   }
 }
@@ -423,7 +338,7 @@ __global__ void __launch_bounds__(512) k_ifx(const GreenArgs A) {
   const C* spec = reinterpret_cast<const C*>(A.spec) + size_t(load) * 3 * size_t(n) * n * nsp;
   // Z[k] = A[k] + i B[k] over the full line, A/B Hermitian-extended; DC/Nyquist imaginary parts dropped
   const int total = nl * n;
-  for (int i = tid; i < total; i += nthr) {
+  batched_copy<4>(tid, nthr, total, [&](int i) {
     const int l = fdiv(i, A.geo.div_n), k = i - l * n;
     C v[2];
 #pragma unroll
@@ -443,8 +358,11 @@ __global__ void __launch_bounds__(512) k_ifx(const GreenArgs A) {
     C z;
     z.x = v[0].x - v[1].y;
     z.y = v[0].y + v[1].x;
+    return z;
+  }, [&](int i, C z) {
+    const int l = fdiv(i, A.geo.div_n), k = i - l * n;
     b0[l * pitch + k] = z;
-  }
+  });
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
   C* res = fft_line<T>(b0, b1, threadIdx.x * pitch, 1, A.plan, tw, true);
@@ -488,7 +406,7 @@ static size_t smem_x(const pgj_ctx* c, size_t cb) {
   return 2 * size_t(nl) * (c->n + 1) * cb + 32 * 3 * 8 + 64;
 }
 static size_t smem_y(const pgj_ctx* c, size_t cb) { return 2 * size_t(c->fg.kcy) * (c->n + 1) * cb; }
-static size_t smem_z(const pgj_ctx* c, size_t cb) { return 2 * 3 * size_t(c->fg.kcz) * (c->n + 1) * cb + 32 * 8 + 64; }
+static size_t smem_z(const pgj_ctx* c, size_t cb) { return 2 * 3 * size_t(c->fg.kcz) * (c->n + 1) * cb + 32 * 4 * 8 + 64; }
 
 template <typename T>
 static int set_smem_limits() {
@@ -557,6 +475,34 @@ int launch_green(pgj_ctx* c, int loads, int prec, const void* r, bool init, cuda
   A.init = init ? 1 : 0;
   A.finalize_fz = 1;
   return prec == PGJ_FP32 ? run_green<float>(c, loads, A, s) : run_green<double>(c, loads, A, s);
+}
+
+// z pass of the slab-fused iteration (DFT(s.r) in the spectrum; mean r subtracted through shat).
+int launch_fz_fused(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s) {
+  GreenArgs A = green_args(c, prec, c->r);
+  A.skip_inactive = 1;
+  A.init = init ? 1 : 0;
+  A.finalize_fz = 1;
+  A.fused = 1;
+  A.shat = c->shat;
+  return prec == PGJ_FP32 ? run_green_pass<float>(c, loads, A, s, 2) : run_green_pass<double>(c, loads, A, s, 2);
+}
+
+// shat = DFT(s) per component (in the context precision), through the x, y and forward z passes on
+// the spectrum of load 0; called whenever the scale field changes.
+int build_shat(pgj_ctx* c, cudaStream_t s) {
+  GreenArgs A = green_args(c, c->prec, c->r);
+  A.skip_inactive = 0;
+  A.use_mean = 0;
+  A.unit_input = 1;
+  A.forward_only = 1;
+  for (int pass = 0; pass < 3; ++pass) {
+    const int st = c->prec == PGJ_FP32 ? run_green_pass<float>(c, 1, A, s, pass) : run_green_pass<double>(c, 1, A, s, pass);
+    if (st) return st;
+  }
+  const size_t bytes = 2 * size_t(c->prec == PGJ_FP32 ? 4 : 8) * 3 * size_t(c->n) * c->n * (c->ns + (c->ns & 1));
+  const cudaError_t e = cudaMemcpyAsync(c->shat, c->spec, bytes, cudaMemcpyDeviceToDevice, s);
+  return e == cudaSuccess ? PGJ_OK : set_cuda_error(e);
 }
 
 // z = P(s . w) = s.w - mean(s.w), from the sw buffer and the IFX finalizer's means.

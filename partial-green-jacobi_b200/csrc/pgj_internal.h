@@ -12,6 +12,7 @@ struct FFTPlan {
   int nst;
   int radix[kMaxStages];
   FastDiv ns_div[kMaxStages];  // stride Ns of each stage (product of the earlier radices)
+  FastDiv nb_div[kMaxStages];  // butterflies per line of each stage (n / radix)
 };
 bool make_fft_plan(int n, FFTPlan* plan);
 
@@ -67,7 +68,7 @@ constexpr int kAuxPartials = 128;
 constexpr int kAuxDoubles = kAuxPartials + kMaxPartials;
 
 struct Layout {
-  size_t a, scale, symbol, symbol32, tw, solutions, f, x, r, p, q, sw, spec, partials, scal, macros,
+  size_t a, scale, symbol, symbol32, tw, solutions, f, x, r, p, q, sw, spec, shat, partials, scal, macros,
       cond, r64, d, aux, total;
 };
 
@@ -101,7 +102,9 @@ struct pgj_ctx {
   void* p;             // (L, 3N) T
   void* q;             // (L, 3N) T
   void* sw;            // (L, 3N) T  s . w (unprojected preconditioned residual)
-  void* spec;          // (L, 3, n, n, ns) complex T
+  void* spec;          // (L, 3, n, n, nsp) complex T
+  void* shat;          // (3, n, n, nsp) complex T: DFT of each component of the scale field
+  int fused;           // PCG iteration as operator + slab-fused update/transform kernels
   double* partials;    // (L, kPartialQ * kMaxPartials)
   pgj::LoadScalars* scal;  // L records used by the kernels being launched (outer or inner)
   pgj::LoadScalars* scal_out;  // certification / FP64 recurrence records
@@ -141,6 +144,15 @@ int launch_green(pgj_ctx* c, int loads, int prec, const void* r, bool init, cuda
 // one Green pass: 0 fft_x, 1 fft_y, 2 fft_z+symbol, 3 ifft_y, 4 ifft_x
 int launch_green_pass(pgj_ctx* c, int loads, int prec, const void* r, bool init, int pass, cudaStream_t s);
 int launch_green_standalone(pgj_ctx* c, int loads, const double* r, double* z, cudaStream_t s);
+int launch_fz_fused(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s);
+int build_shat(pgj_ctx* c, cudaStream_t s);
+// slab-fused iteration (pgj_slab.cu)
+enum SlabLaunch { kSlabUpdateL = 0, kSlabInitL = 1, kSlabSyncL = 2 };
+bool slab_fits(const pgj_ctx* c);
+int prepare_slab_kernels();
+int launch_fxy(pgj_ctx* c, int loads, int prec, int mode, void* u, cudaStream_t s);
+int launch_ifxy(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, cudaGraphConditionalHandle h,
+                bool set_cond);
 // pcg (pgj_pcg.cu)
 int launch_update_ur(pgj_ctx* c, int loads, int prec, double* u64, void* uT, cudaStream_t s);
 int launch_update_p(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, cudaGraphConditionalHandle h,

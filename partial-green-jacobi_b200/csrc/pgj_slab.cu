@@ -1,0 +1,366 @@
+// Slab-fused PCG iteration: the vector updates of the recurrence fused with the x/y transforms of
+// the Green apply, so that one iteration is four kernels over the DOF vectors and the spectrum:
+//
+//   operator : q = K p, alpha = rz / p.q                         (pgj_operator.cu)
+//   fxy      : u += alpha p, r -= alpha q, ||r||^2, sum r  -> last block: masks, mean r;
+//              2D real DFT over (x, y) of s.r for one (load, component, z) slab    (this file)
+//   fz       : DFT along z, - mean r . DFT(s), symbol, <v, G v> and mean(s.w) by Parseval,
+//              inverse along z -> last block: rz, beta, mean(s.w)                   (pgj_fft.cu)
+//   ifxy     : inverse y and C2R x of the slab, p = (s.w - mean(s.w)) + beta p      (this file)
+//
+// Same recurrence as resident.py:119-131 of exp/asg_gpu_resident_20261103 (the unfused kernels in
+// pgj_pcg.cu and the five-pass Green apply in pgj_fft.cu do it step by step); the two means of the
+// projection P are exact linear identities moved into the spectral pass:
+//   DFT(s.(r - m)) = DFT(s.r) - m DFT(s),   sum_x s.w = sum_k W(k) conj(DFT(s)(k)).
+// A block owns one component of one z-plane: an n x n real slab, two rows packed per complex
+// line for the real transform, the half spectrum as n rows of nsp (even) complex values.
+#include "pgj_fft_engine.cuh"
+#include <cstring>
+
+namespace pgj {
+
+enum SlabMode { kSlabUpdate = 0, kSlabInit = 1, kSlabSync = 2 };
+
+struct SlabArgs {
+  int n, ns, nsp;
+  FFTPlan plan;
+  FastDiv div_n, div_ns;
+  void* p;                // (L,3N) T search directions
+  const void* q;          // (L,3N) T K p
+  void* r;                // (L,3N) T recurrence residual
+  void* u;                // (L,3N) U iterate (FP64 x, or the FP32 correction d)
+  const double* r64;      // sync mode: FP64 true residual
+  const double* scale;    // (3N) FP64 scale field s
+  void* spec;             // (L,3,n,n,nsp) complex T
+  const void* tw;         // n complex T twiddles
+  LoadScalars* scal;      // recurrence records
+  const LoadScalars* out; // sync mode: certificate records (res2, mean r of the true residual)
+  double* partials;
+  int cap;
+  double rel_delta2;
+  int loads;
+  int init;               // ifxy: p = P(s.w) (first direction)
+  int set_cond;           // ifxy: set the WHILE condition (any load active, bounded body count)
+  cudaGraphConditionalHandle h;
+  int* counters;
+};
+
+constexpr int kMaxBodyRunsSlab = 4100;  // same bound as the unfused loop body
+
+template <typename T>
+__device__ __forceinline__ T* real_view(cplx<T>* b) { return reinterpret_cast<T*>(b); }
+
+// ------------------------------------------------------------------------------------------ fxy
+template <typename T, typename U, int MODE>
+__global__ void __launch_bounds__(512, 2) k_fxy(const SlabArgs A) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int c = blockIdx.x, z = blockIdx.y, load = blockIdx.z;
+  LoadScalars& S = A.scal[load];
+  if (MODE == kSlabSync ? (S.reliable == 0) : (S.active == 0)) return;
+  const int n = A.n, ns = A.ns, nsp = A.nsp;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int nn = n * n;
+  C* b0 = reinterpret_cast<C*>(smem_raw);
+  C* b1 = b0 + size_t(n) * nsp;
+  double* red = reinterpret_cast<double*>(b1 + size_t(n) * nsp);
+  const size_t N = size_t(nn) * n, N3 = 3 * N;
+  const size_t node0 = size_t(z) * nn;
+  const size_t off = size_t(load) * N3 + 3 * node0 + c;  // dof of node (0,0,z), component c
+  T* r = reinterpret_cast<T*>(A.r) + off;
+  const double* sc = A.scale + 3 * node0 + c;
+  T* packed = real_view<T>(b0);
+  double acc[2] = {0.0, 0.0};
+  const double alpha = MODE == kSlabUpdate ? S.alpha : 0.0;
+  const T a = T(alpha);
+  // nodes whose loads are in flight together (the FP64 update keeps five doubles per node)
+  constexpr int UNR = (MODE == kSlabUpdate && sizeof(T) == 8) ? 2 : 4;
+  const T* pg = reinterpret_cast<const T*>(A.p) + off;
+  const T* qg = reinterpret_cast<const T*>(A.q) + off;
+  U* ug = reinterpret_cast<U*>(A.u) + off;
+  const double* r64 = A.r64 + off;
+  for (int i0 = tid; i0 < nn; i0 += UNR * nthr) {
+    // all loads of UNR nodes first, then the updates and stores
+    T pv[UNR], qv[UNR], rv[UNR];
+    U uv[UNR];
+    double sv[UNR];
+#pragma unroll
+    for (int j = 0; j < UNR; ++j) {
+      const int i = i0 + j * nthr;
+      if (i < nn) {
+        const size_t k = 3 * size_t(i);
+        sv[j] = sc[k];
+        if (MODE == kSlabUpdate) { pv[j] = pg[k]; qv[j] = qg[k]; rv[j] = r[k]; uv[j] = ug[k]; }
+        else if (MODE == kSlabSync) rv[j] = T(r64[k]);
+        else rv[j] = r[k];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < UNR; ++j) {
+      const int i = i0 + j * nthr;
+      if (i < nn) {
+        const size_t k = 3 * size_t(i);
+        const int y = fdiv(i, A.div_n), x = i - y * n;
+        T rj = rv[j];
+        if (MODE == kSlabUpdate) {
+          ug[k] = uv[j] + U(alpha) * U(pv[j]);
+          rj = rj - a * qv[j];
+          r[k] = rj;
+          const double rd = double(rj);
+          acc[0] += rd * rd;
+          acc[1] += rd;
+        } else if (MODE == kSlabSync) {
+          r[k] = rj;
+        }
+        // rows 2l and 2l+1 packed as the real and imaginary parts of complex line l (offset 2 l nsp)
+        packed[2 * ((y >> 1) * 2 * nsp + x) + (y & 1)] = T(sv[j]) * rj;
+      }
+    }
+  }
+  __syncthreads();
+  const C* tw = reinterpret_cast<const C*>(A.tw);
+  C* res = fft_lines<T, false>(b0, b1, n / 2, 2 * nsp, 1, A.plan, A.div_n, tw, false, tid, nthr);
+  C* oth = res == b0 ? b1 : b0;
+  // split the packed transforms: row rho = 2l (real part) and 2l+1 (imaginary part)
+  for (int i = tid; i < n * ns; i += nthr) {
+    const int rho = fdiv(i, A.div_ns), k = i - rho * ns;
+    const C* line = res + (rho >> 1) * 2 * nsp;
+    const C zk = line[k];
+    const C zn = line[k == 0 ? 0 : n - k];
+    C o;
+    if ((rho & 1) == 0) { o.x = T(0.5) * (zk.x + zn.x); o.y = T(0.5) * (zk.y - zn.y); }
+    else { o.x = T(0.5) * (zk.y + zn.y); o.y = T(0.5) * (zn.x - zk.x); }
+    oth[rho * nsp + k] = o;
+  }
+  __syncthreads();
+  // y transform of the ns columns
+  C* res2 = fft_lines<T, true>(oth, res, ns, 1, nsp, A.plan, A.div_ns, tw, false, tid, nthr);
+  C* sp = reinterpret_cast<C*>(A.spec) + ((size_t(load) * 3 + c) * n + z) * size_t(n) * nsp;
+  for (int i = tid; i < n * ns; i += nthr) {
+    const int ky = fdiv(i, A.div_ns), kx = i - ky * ns;
+    sp[size_t(ky) * nsp + kx] = res2[ky * nsp + kx];
+  }
+  if (MODE == kSlabInit) return;
+
+  const int nblk = 3 * n, blk = c + 3 * z;
+  double* part = A.partials + size_t(load) * kPartialQ * kMaxPartials;
+  if (MODE == kSlabUpdate) {
+    block_sum<2>(acc, red);
+    if (tid == 0) {
+      part[blk] = acc[0];
+      for (int cc = 0; cc < 3; ++cc) part[(1 + cc) * kMaxPartials + blk] = cc == c ? acc[1] : 0.0;
+    }
+    if (!last_block(&S.ticket[kTicketUpdate], nblk)) return;
+    if (tid < 32) {
+      double v[4];
+      for (int k = 0; k < 4; ++k) v[k] = warp_sum_partials(part + k * kMaxPartials, nblk);
+      if (tid == 0) {
+        // same bookkeeping as the unfused update (k_update_ur)
+        const double res2 = v[0];
+        const bool finite = isfinite(res2);
+        const int it = S.iterations + 1;
+        const bool valid = S.failed == 0;
+        const bool keep = valid && finite && (res2 > S.target2) && (it < A.cap);
+        S.iterations = it;
+        S.bad = S.bad | (valid ? 0 : 1) | (finite ? 0 : 1);
+        S.active = keep ? 1 : 0;
+        S.res2 = res2;
+        for (int cc = 0; cc < 3; ++cc) S.mean_r[cc] = v[1 + cc] / double(N);
+        if (A.rel_delta2 > 0.0) {
+          const bool ok = valid && finite && it < A.cap;
+          S.reliable = ok && ((keep && res2 < A.rel_delta2 * S.anchor) || (!keep && res2 <= S.target2)) ? 1 : 0;
+        }
+      }
+    }
+  } else {  // kSlabSync: the recurrence restarts from the FP64 true residual (k_rel_sync)
+    if (!last_block(&S.ticket[kTicketAux2], nblk)) return;
+    if (tid == 0) {
+      const LoadScalars& O = A.out[load];
+      S.res2 = O.res2;
+      S.anchor = O.res2;
+      for (int cc = 0; cc < 3; ++cc) S.mean_r[cc] = O.mean_r[cc];
+      S.active = isfinite(O.res2) && O.res2 > S.target2 && S.iterations < A.cap && !S.bad ? 1 : 0;
+      S.reliable = 0;
+    }
+  }
+}
+
+// ----------------------------------------------------------------------------------------- ifxy
+template <typename T>
+__global__ void __launch_bounds__(512, 2) k_ifxy(const SlabArgs A) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int c = blockIdx.x, z = blockIdx.y, load = blockIdx.z;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  if (A.set_cond && c == 0 && z == 0 && load == 0 && tid == 0) {
+    int any = 0;
+    for (int l = 0; l < A.loads; ++l) any |= A.scal[l].active;
+    const int runs = ++A.counters[0];
+    A.counters[5] += 1;                                 // loop bodies over the whole solve
+    if (runs >= kMaxBodyRunsSlab) A.counters[1] = 1;  // recorded: loop stopped by the bound
+    cudaGraphSetConditional(A.h, (any && runs < kMaxBodyRunsSlab) ? 1u : 0u);
+  }
+  const LoadScalars& S = A.scal[load];
+  if (!S.active) return;
+  const int n = A.n, ns = A.ns, nsp = A.nsp;
+  const int nn = n * n;
+  C* b0 = reinterpret_cast<C*>(smem_raw);
+  C* b1 = b0 + size_t(n) * nsp;
+  const C* sp = reinterpret_cast<const C*>(A.spec) + ((size_t(load) * 3 + c) * n + z) * size_t(n) * nsp;
+  batched_copy<8>(tid, nthr, n * ns, [&](int i) {
+    const int ky = fdiv(i, A.div_ns), kx = i - ky * ns;
+    return sp[size_t(ky) * nsp + kx];
+  }, [&](int i, C v) {
+    const int ky = fdiv(i, A.div_ns), kx = i - ky * ns;
+    b0[ky * nsp + kx] = v;
+  });
+  __syncthreads();
+  const C* tw = reinterpret_cast<const C*>(A.tw);
+  C* res = fft_lines<T, true>(b0, b1, ns, 1, nsp, A.plan, A.div_ns, tw, true, tid, nthr);
+  C* oth = res == b0 ? b1 : b0;
+  // C2R packing: line l = A + i B over the full x range (rows 2l, 2l+1 Hermitian-extended,
+  // imaginary parts of the DC and Nyquist bins dropped)
+  for (int i = tid; i < (n / 2) * n; i += nthr) {
+    const int l = fdiv(i, A.div_n), k = i - l * n;
+    C v[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const C* row = res + (2 * l + h) * nsp;
+      C val;
+      if (k < ns) {
+        val = row[k];
+        if (k == 0 || k == n / 2) val.y = T(0);
+      } else {
+        val = cconj(row[n - k]);
+      }
+      v[h] = val;
+    }
+    C zz;
+    zz.x = v[0].x - v[1].y;
+    zz.y = v[0].y + v[1].x;
+    oth[l * 2 * nsp + k] = zz;
+  }
+  __syncthreads();
+  C* res2 = fft_lines<T, false>(oth, res, n / 2, 2 * nsp, 1, A.plan, A.div_n, tw, true, tid, nthr);
+  const T* wv = real_view<T>(res2);
+  const size_t node0 = size_t(z) * nn;
+  const size_t off = size_t(load) * 3 * size_t(nn) * n + 3 * node0 + c;
+  T* p = reinterpret_cast<T*>(A.p) + off;
+  const double* sc = A.scale + 3 * node0 + c;
+  const T m = T(S.mean_z[c]);
+  const T beta = T(S.beta);
+  constexpr int UNR = 4;
+  for (int i0 = tid; i0 < nn; i0 += UNR * nthr) {
+    T pv[UNR];
+    double sv[UNR];
+#pragma unroll
+    for (int j = 0; j < UNR; ++j) {
+      const int i = i0 + j * nthr;
+      if (i < nn) {
+        const size_t k = 3 * size_t(i);
+        sv[j] = sc[k];
+        pv[j] = A.init ? T(0) : p[k];
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < UNR; ++j) {
+      const int i = i0 + j * nthr;
+      if (i < nn) {
+        const int y = fdiv(i, A.div_n), x = i - y * n;
+        const T w = wv[2 * ((y >> 1) * 2 * nsp + x) + (y & 1)];
+        const T zv = T(sv[j]) * w - m;
+        p[3 * size_t(i)] = A.init ? zv : zv + beta * pv[j];
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------ host side
+static size_t slab_smem(int n, int nsp, size_t tsz) { return 2 * size_t(n) * nsp * 2 * tsz + 32 * 2 * 8 + 64; }
+
+static int slab_threads(const pgj_ctx* c) {
+  int minr = 8;
+  for (int i = 0; i < c->plan.nst; ++i) minr = c->plan.radix[i] < minr ? c->plan.radix[i] : minr;
+  const int ns = c->ns;
+  int w = (ns * c->n) / minr;  // butterflies of the widest stage over the y columns
+  int t = ((w + 31) / 32) * 32;
+  if (t > 512) t = 512;
+  if (t < 64) t = 64;
+  return t;
+}
+
+bool slab_fits(const pgj_ctx* c) {
+  const size_t tsz = c->prec == PGJ_FP32 ? 4 : 8;
+  const int nsp = c->ns + (c->ns & 1);
+  return slab_smem(c->n, nsp, tsz) <= 110 * 1024;  // two blocks per SM
+}
+
+int prepare_slab_kernels() {
+  const int lim = 112 * 1024;
+  cudaFuncSetAttribute(k_fxy<double, double, kSlabUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<double, double, kSlabInit>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<double, double, kSlabSync>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<float, float, kSlabUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<float, float, kSlabInit>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<float, float, kSlabSync>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_ifxy<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_ifxy<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  return check_launch();
+}
+
+static SlabArgs slab_args(pgj_ctx* c, int loads, int prec) {
+  SlabArgs A;
+  std::memset(&A, 0, sizeof(A));
+  A.n = c->n; A.ns = c->ns; A.nsp = c->ns + (c->ns & 1);
+  A.plan = c->plan;
+  A.div_n = make_fastdiv(unsigned(c->n));
+  A.div_ns = make_fastdiv(unsigned(c->ns));
+  A.p = c->p; A.q = c->q; A.r = c->r;
+  A.r64 = c->r64; A.scale = c->scale; A.spec = c->spec;
+  A.tw = prec == PGJ_FP32 ? static_cast<const void*>(static_cast<double2*>(c->tw) + c->n) : c->tw;
+  A.scal = c->scal; A.out = c->scal_out; A.partials = c->partials;
+  A.cap = 4000; A.rel_delta2 = c->rel_delta2; A.loads = loads;
+  A.counters = c->cond;
+  return A;
+}
+
+// mode: kSlabUpdate (u in `u`: FP64 x, or the FP32 correction d), kSlabInit, kSlabSync
+int launch_fxy(pgj_ctx* c, int loads, int prec, int mode, void* u, cudaStream_t s) {
+  SlabArgs A = slab_args(c, loads, prec);
+  A.u = u;
+  const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
+  const dim3 grid(3, c->n, loads);
+  const int thr = slab_threads(c);
+  const size_t smem = slab_smem(A.n, A.nsp, tsz);
+  if (prec == PGJ_FP32) {
+    switch (mode) {
+      case kSlabUpdate: k_fxy<float, float, kSlabUpdate><<<grid, thr, smem, s>>>(A); break;
+      case kSlabInit: k_fxy<float, float, kSlabInit><<<grid, thr, smem, s>>>(A); break;
+      default: k_fxy<float, float, kSlabSync><<<grid, thr, smem, s>>>(A); break;
+    }
+  } else {
+    switch (mode) {
+      case kSlabUpdate: k_fxy<double, double, kSlabUpdate><<<grid, thr, smem, s>>>(A); break;
+      case kSlabInit: k_fxy<double, double, kSlabInit><<<grid, thr, smem, s>>>(A); break;
+      default: k_fxy<double, double, kSlabSync><<<grid, thr, smem, s>>>(A); break;
+    }
+  }
+  return check_launch();
+}
+
+int launch_ifxy(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, cudaGraphConditionalHandle h,
+                bool set_cond) {
+  SlabArgs A = slab_args(c, loads, prec);
+  A.init = init ? 1 : 0;
+  A.set_cond = set_cond ? 1 : 0;
+  A.h = h;
+  const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
+  const dim3 grid(3, c->n, loads);
+  const int thr = slab_threads(c);
+  const size_t smem = slab_smem(A.n, A.nsp, tsz);
+  if (prec == PGJ_FP32) k_ifxy<float><<<grid, thr, smem, s>>>(A);
+  else k_ifxy<double><<<grid, thr, smem, s>>>(A);
+  return check_launch();
+}
+
+}  // namespace pgj

@@ -218,8 +218,19 @@ class Operator:
         nbytes = (C.c_double * 8)()
         _lib.check(_lib.lib().pgj_profile_iteration(self._ctx, m.shape[0], m.ctypes.data, int(reps), ms, nbytes,
                                                     _stream_ptr()), "pgj_profile_iteration")
-        names = ["operator", "update_ur", "fft_x", "fft_y", "fft_z_symbol", "ifft_y", "ifft_x", "update_p"]
+        if self.fused_iteration:
+            names = ["operator", "update_fft_xy", "fft_z_symbol", "ifft_xy_update_p"]
+        else:
+            names = ["operator", "update_ur", "fft_x", "fft_y", "fft_z_symbol", "ifft_y", "ifft_x", "update_p"]
         return {k: dict(ms=ms[i], bytes=nbytes[i]) for i, k in enumerate(names)}
+
+    @property
+    def fused_iteration(self) -> bool:
+        """True when one PCG iteration runs as four kernels (slab-fused updates and transforms)."""
+        return bool(_lib.lib().pgj_fused_iteration(self._ctx))
+
+    def set_fused_iteration(self, on: bool) -> None:
+        _lib.check(_lib.lib().pgj_set_fused_iteration(self._ctx, 1 if on else 0), "pgj_set_fused_iteration")
 
     def energies(self, u, macros):
         torch = _torch()

@@ -313,8 +313,41 @@ def test_profile_iteration_reports_all_kernels(pkg):
         op = pkg.Operator(n, 6, *pkg.PAPER_MEDIUM, precision=prec)
         op.set_material(dev(pkg.baseline_design(n, seed=1, emin=1e-6)))
         op.set_alpha(0.5)
-        prof = op.profile_iteration(np.eye(6), reps=3)
-        assert len(prof) == 8 and all(v["ms"] > 0 and v["bytes"] > 0 for v in prof.values())
+        for fused in (True, False):
+            op.set_fused_iteration(fused)
+            prof = op.profile_iteration(np.eye(6), reps=3)
+            assert len(prof) == (4 if fused else 8)
+            assert all(v["ms"] > 0 and v["bytes"] > 0 for v in prof.values()), prof
+
+
+@pytest.mark.parametrize("n,prec,emin", [(12, "fp64", 1e-6), (30, "fp64", 1e-4), (16, "mixed", 1e-6),
+                                         (20, "mixed", 1e-9)])
+def test_fused_iteration_matches_unfused(pkg, n, prec, emin):
+    """Four-kernel iteration (updates fused with the slab transforms, projection means by Parseval)
+    against the step-by-step kernels: same iteration counts, same C_H."""
+    lam, mu = pkg.PAPER_MEDIUM
+    a = dev(pkg.baseline_design(n, seed=21, emin=emin))
+    out = {}
+    for fused in (False, True):
+        op = pkg.Operator(n, 6, lam, mu, precision=prec)
+        op.set_fused_iteration(fused)
+        assert op.fused_iteration == fused
+        op.set_material(a)
+        op.set_alpha(0.5)
+        u = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")
+        infos, st = op.solve(np.eye(6), 1e-8, u)
+        assert st == 0, (fused, infos)
+        out[fused] = (op.effective_tensor(u).cpu().numpy(), np.array([i["iterations"] for i in infos]))
+    (C0, i0), (C1, i1) = out[False], out[True]
+    assert np.all(np.abs(i1 - i0) <= np.maximum(1, np.ceil(0.02 * i0))), (i0, i1)
+    assert rel(C1, C0) < (1e-10 if prec == "fp64" else 1e-7), rel(C1, C0)
+
+
+def test_fused_iteration_falls_back_when_the_slab_does_not_fit(pkg):
+    op = pkg.Operator(128, 1, *pkg.PAPER_MEDIUM)
+    assert not op.fused_iteration
+    with pytest.raises(RuntimeError, match="unsupported"):
+        op.set_fused_iteration(True)
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
