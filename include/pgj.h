@@ -156,6 +156,11 @@ int pgj_profile_iteration(pgj_ctx* ctx, int loads, const double* macros, int rep
 int pgj_fused_iteration(pgj_ctx* ctx);
 int pgj_set_fused_iteration(pgj_ctx* ctx, int on);
 
+/* Tile shapes the context's autotuners picked (no reference counterpart): out[0] operator rows per
+ * block, out[1] operator z-planes per block, out[2] rows per x-pass block, out[3] / out[4] kx columns
+ * per y / z-pass block, out[5] fused iteration flag. */
+int pgj_tile_shapes(pgj_ctx* ctx, int* out);
+
 /* Failure-detection self-test (no reference counterpart): runs the bounded device wait used by the
  * kernels' TMA staging on an mbarrier that nothing completes, giving up after `tries` polls.
  * Returns PGJ_ERR_TIMEOUT when the wait expired and was reported (the expected outcome); the

@@ -67,6 +67,7 @@ SIGNATURES = {
     "pgj_last_launches": (C.c_longlong, [vp]),
     "pgj_selftest_wait_timeout": (C.c_int, [vp, C.c_int, vp]),
     "pgj_fused_iteration": (C.c_int, [vp]),
+    "pgj_tile_shapes": (C.c_int, [vp, C.POINTER(C.c_int)]),
     "pgj_set_fused_iteration": (C.c_int, [vp, C.c_int]),
     "pgj_profile_iteration": (C.c_int, [vp, C.c_int, vp, C.c_int, vp, vp, vp]),
     "pgj_energies": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),

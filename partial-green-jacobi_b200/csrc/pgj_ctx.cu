@@ -704,6 +704,13 @@ long long pgj_last_launches(pgj_ctx* c) { return c ? c->last_launches : -1; }
 
 int pgj_fused_iteration(pgj_ctx* c) { return c ? c->fused : -1; }
 
+int pgj_tile_shapes(pgj_ctx* c, int* out) {
+  if (!c || !out) return PGJ_ERR_ARGUMENT;
+  out[0] = c->sg.ty; out[1] = c->sg.zc; out[2] = c->fg.rb; out[3] = c->fg.kcy; out[4] = c->fg.kcz;
+  out[5] = c->fused;
+  return PGJ_OK;
+}
+
 int pgj_set_fused_iteration(pgj_ctx* c, int on) {
   if (!c || (on != 0 && on != 1)) return PGJ_ERR_ARGUMENT;
   if (on && !slab_fits(c)) return PGJ_ERR_UNSUPPORTED;

@@ -561,18 +561,24 @@ int autotune_fft(pgj_ctx* c, cudaStream_t s) {
   cudaEventCreate(&e1);
   FFTGeom best = c->fg;
   float best_ms = 1e30f;
+  for (int r = 0; r < 10; ++r)  // bring the clocks up before timing anything
+    c->prec == PGJ_FP32 ? run_green<float>(c, c->L, A, s) : run_green<double>(c, c->L, A, s);
   for (const FFTGeom& g : cands) {
     c->fg = g;
     A.geo = g;
     int st = c->prec == PGJ_FP32 ? run_green<float>(c, c->L, A, s) : run_green<double>(c, c->L, A, s);
     if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); c->fg = best; return st; }
-    cudaEventRecord(e0, s);
-    for (int r = 0; r < 3; ++r)
-      c->prec == PGJ_FP32 ? run_green<float>(c, c->L, A, s) : run_green<double>(c, c->L, A, s);
-    cudaEventRecord(e1, s);
-    cudaEventSynchronize(e1);
-    float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
+    float ms = 1e30f;
+    for (int trial = 0; trial < 2; ++trial) {  // best of two trials of three applies
+      cudaEventRecord(e0, s);
+      for (int r = 0; r < 3; ++r)
+        c->prec == PGJ_FP32 ? run_green<float>(c, c->L, A, s) : run_green<double>(c, c->L, A, s);
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      float t = 0.f;
+      cudaEventElapsedTime(&t, e0, e1);
+      ms = t < ms ? t : ms;
+    }
     if (ms < best_ms) { best_ms = ms; best = g; }
   }
   cudaEventDestroy(e0);

@@ -22,10 +22,11 @@ struct StencilGeom {
   int ntiles;  // tiles along y
   int zc;      // output node planes per block
   int nchunks; // chunks along z
-  int threads() const { return 0; }
+  int stages;  // node-plane buffers of the TMA staging pipeline (2..4)
+  int occ;     // 1: up to 512 threads per block; 3: at most 256 threads, three blocks per SM
 };
 StencilGeom stencil_geom(int n, int loads);
-StencilGeom stencil_geom_shape(int n, int ty, int zc);
+StencilGeom stencil_geom_shape(int n, int ty, int zc, int stages = 2, int occ = 1);
 
 // Geometry of the FFT passes.
 struct FFTGeom {
@@ -55,6 +56,7 @@ struct StencilArgs {
   OpConst kc;
   int iteration_cap;
   int tma;                     // stage planes with bulk async copies (aligned rows) instead of cp.async
+  int stages;                  // plane buffers in the staging pipeline
   int* err;                    // set to 1 if a bounded device wait expired
 };
 

@@ -20,6 +20,8 @@
 
 namespace pgj {
 
+constexpr int kMaxPlaneStages = 4;  // node-plane buffers of the operator's staging pipeline (upper bound)
+
 template <typename T> __device__ __forceinline__ void cp_async(T* dst, const T* src);
 template <> __device__ __forceinline__ void cp_async<double>(double* dst, const double* src) {
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(smem_u32(dst)), "l"(src));
@@ -43,12 +45,14 @@ __device__ __forceinline__ void tma_plane(T* buf, const T* in, int pz, int y0, i
   }
 }
 
-StencilGeom stencil_geom_shape(int n, int ty, int zc) {
+StencilGeom stencil_geom_shape(int n, int ty, int zc, int stages, int occ) {
   StencilGeom g;
+  g.occ = occ;
   g.ty = ty;
   g.ntiles = (n + ty - 1) / ty;
   g.zc = zc;
   g.nchunks = (n + zc - 1) / zc;
+  g.stages = stages;
   return g;
 }
 
@@ -79,6 +83,13 @@ StencilGeom stencil_geom(int n, int loads) {
     if (v >= 1 && v <= n) g.zc = v;
   }
   g.nchunks = (n + g.zc - 1) / g.zc;
+  g.stages = 2;
+  if (const char* e = std::getenv("PGJ_STENCIL_STAGES")) {
+    const int v = std::atoi(e);
+    if (v >= 2 && v <= kMaxPlaneStages) g.stages = v;
+  }
+  g.occ = 1;
+  if (const char* e = std::getenv("PGJ_STENCIL_OCC")) g.occ = std::atoi(e) == 3 ? 3 : 1;
   return g;
 }
 
@@ -115,8 +126,10 @@ __device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, 
   }
 }
 
-template <typename T, int MODE>
-__global__ void __launch_bounds__(512, 1) k_stencil(const StencilArgs A) {
+// OCC = 1: blocks of up to 512 threads, registers unconstrained (128); OCC = 3: blocks of at most
+// 256 threads, three resident per SM (85 registers).
+template <typename T, int MODE, int OCC>
+__global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const StencilArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = A.n, TY = A.ty;
   const int tx = threadIdx.x, ty = threadIdx.y;
@@ -146,36 +159,38 @@ __global__ void __launch_bounds__(512, 1) k_stencil(const StencilArgs A) {
   }
   const T* in = reinterpret_cast<const T*>(A.in) + size_t(load) * 3 * N;
 
+  // plane j (node plane z0 - 1 + j) sits in buffer j % NS; TMA staging keeps NS - 1 planes in flight,
+  // the cp.async fallback two
+  const int NS = A.tma ? A.stages : 2;
   const int planevals = (TY + 2) * 3 * n;
-  T* buf0 = reinterpret_cast<T*>(smem_raw);
-  T* buf1 = buf0 + planevals;
-  T* upy = buf1 + planevals;              // (TY+1) * n * 6
+  T* bufs = reinterpret_cast<T*>(smem_raw);
+  T* upy = bufs + NS * planevals;          // (TY+1) * n * 6
   T* upx = upy + (TY + 1) * n * 6;         // (TY+1) * n * 3
   double* red = reinterpret_cast<double*>(upx + (TY + 1) * n * 3 + 2);  // 32 * 4, 16-byte padded
   red = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(red) + 15) & ~uintptr_t(15));
-  uint64_t* bars = reinterpret_cast<uint64_t*>(red + 32 * 4);  // two mbarriers (TMA staging)
+  uint64_t* bars = reinterpret_cast<uint64_t*>(red + 32 * 4);  // NS mbarriers (TMA staging)
   const bool tma = A.tma != 0;
+  const int nplanes = zc + 2;
+  T* buf0 = bufs;
 
-  // prologue: planes z0-1 (j = 0, buffer 0) and z0 (j = 1, buffer 1)
+  // prologue: planes j = 0 .. NS-1 (plane 0 is z0 - 1)
   if (tma) {
     if (tid == 0) {
-      mbar_init(&bars[0], 1);
-      mbar_init(&bars[1], 1);
+      for (int b = 0; b < NS; ++b) mbar_init(&bars[b], 1);
       fence_mbar_init();
     }
     __syncthreads();
-    if (tid == 0) {
-      tma_plane(buf0, in, (z0 - 1 + n) % n, y0, TY + 2, n, &bars[0]);
-      tma_plane(buf1, in, z0 % n, y0, TY + 2, n, &bars[1]);
-    }
-    const bool okw = mbar_wait(&bars[0], 0);
+    if (tid == 0)
+      for (int j = 0; j < NS && j < nplanes; ++j)
+        tma_plane(bufs + j * planevals, in, (z0 - 1 + j + n) % n, y0, TY + 2, n, &bars[j]);
+    const bool okw = tid == 0 ? mbar_wait(&bars[0], 0) : true;
     if (__syncthreads_or(!okw)) {
       if (tid == 0 && A.err) atomicExch(A.err, 1);
       return;
     }
   } else {
-    stage_plane(buf0, in, (z0 - 1 + n) % n, y0, TY + 2, n, tid, nthr);
-    stage_plane(buf1, in, z0 % n, y0, TY + 2, n, tid, nthr);
+    stage_plane(bufs, in, (z0 - 1 + n) % n, y0, TY + 2, n, tid, nthr);
+    stage_plane(bufs + planevals, in, z0 % n, y0, TY + 2, n, tid, nthr);
     cp_wait_one();
     __syncthreads();
   }
@@ -192,24 +207,41 @@ __global__ void __launch_bounds__(512, 1) k_stencil(const StencilArgs A) {
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   const double* aa = A.a;
 
+  // element densities are read one plane ahead so their latency overlaps the previous plane
+  const double* arow = aa + size_t(eyw) * n + tx;
+  const size_t aplane = size_t(n) * n;
+  int za = (z0 - 1 + n) % n;  // element plane of the next density read (wraps incrementally)
+  double a_next = __ldg(arow + size_t(za) * aplane);
+  // buffer / phase bookkeeping without divisions: plane j = s + 1 sits in buffer jb with mbarrier
+  // parity jpar; plane s (refilled with plane s + NS) in buffer sb; zr = node plane s + NS (mod n)
+  int jb = 1 % NS, sb = 0;
+  unsigned jpar = 0u;
+  int zr = (z0 - 1 + NS) % n;
   for (int s = 0; s <= zc; ++s) {
     const int ez = z0 - 1 + s;           // element plane
-    const int ezw = (ez + n) % n;
-    const T ae = T(__ldg(aa + (size_t(ezw) * n + eyw) * n + tx));
-    T* cur = ((s + 1) & 1) ? buf1 : buf0;
+    const T ae = T(a_next);
+    if (s < zc) {
+      za = za + 1 == n ? 0 : za + 1;
+      a_next = __ldg(arow + size_t(za) * aplane);
+    }
+    T* cur = bufs + jb * planevals;
     if (tma) {
-      // plane j = s + 1 sits in buffer (s+1)&1, use number (s+1)>>1
-      const bool okw = mbar_wait(&bars[(s + 1) & 1], ((s + 1) >> 1) & 1);
+      // one thread observes the plane's arrival (acquire); the block barrier publishes it
+      const bool okw = tid == 0 ? mbar_wait(&bars[jb], jpar) : true;
       if (__syncthreads_or(!okw)) {
         if (tid == 0 && A.err) atomicExch(A.err, 1);
         return;
       }
-      if (s < zc && tid == 0) tma_plane(((s & 1) ? buf1 : buf0), in, (z0 + s + 1) % n, y0, TY + 2, n, &bars[s & 1]);
+      // plane s was consumed by the previous step: refill its buffer with plane s + NS
+      if (tid == 0 && s + NS < nplanes) tma_plane(bufs + sb * planevals, in, zr, y0, TY + 2, n, &bars[sb]);
     } else {
       cp_wait_all();
       __syncthreads();
-      if (s < zc) stage_plane(((s & 1) ? buf1 : buf0), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
+      if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
     }
+    if (++jb == NS) { jb = 0; jpar ^= 1u; }
+    sb = sb + 1 == NS ? 0 : sb + 1;
+    zr = zr + 1 == n ? 0 : zr + 1;
 
     T F1[4][3], own1[3];
     face_modes(cur, ty, tx, n, F1, own1);
@@ -337,7 +369,8 @@ int autotune_stencil(pgj_ctx* c, cudaStream_t s) {
     auto it = g_tuned.find(key);
     if (it != g_tuned.end()) { c->sg = it->second; return PGJ_OK; }
   }
-  if (std::getenv("PGJ_STENCIL_TY") || std::getenv("PGJ_STENCIL_ZC")) return PGJ_OK;  // manual override
+  if (std::getenv("PGJ_STENCIL_TY") || std::getenv("PGJ_STENCIL_ZC") || std::getenv("PGJ_STENCIL_OCC"))
+    return PGJ_OK;  // manual override
   std::vector<int> tys;
   for (int ty : {1, 2, 3, 4, 5, 6, 7, 8, 12, 16, 31})
     if (ty <= n && n * (ty + 1) <= 512 && (ty + 1) * n >= 32) tys.push_back(ty);
@@ -352,21 +385,30 @@ int autotune_stencil(pgj_ctx* c, cudaStream_t s) {
   float best_ms = 1e30f;
   const void* in = c->p;
   void* out = c->q;
+  // bring the clocks up before timing anything
+  for (int r = 0; r < 30; ++r) launch_stencil(c, kPlain, c->L, c->prec, in, out, nullptr, nullptr, s);
   for (int ty : tys)
-    for (int zc : zcs) {
-      StencilGeom g = stencil_geom_shape(n, ty, zc);
-      if (g.ntiles * g.nchunks > kMaxPartials) continue;
-      c->sg = g;
-      int st = launch_stencil(c, kPlain, c->L, c->prec, in, out, nullptr, nullptr, s);  // warm
-      if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
-      cudaEventRecord(e0, s);
-      for (int r = 0; r < 3; ++r) launch_stencil(c, kPlain, c->L, c->prec, in, out, nullptr, nullptr, s);
-      cudaEventRecord(e1, s);
-      cudaEventSynchronize(e1);
-      float ms = 0.f;
-      cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best_ms) { best_ms = ms; best = g; }
-    }
+    for (int zc : zcs)
+      for (int occ : {1, 3})
+      for (int stages = 2; stages <= kMaxPlaneStages; stages += 2) {
+        if (occ == 3 && n * (ty + 1) > 256) continue;
+        StencilGeom g = stencil_geom_shape(n, ty, zc, stages, occ);
+        if (g.ntiles * g.nchunks > kMaxPartials) continue;
+        c->sg = g;
+        int st = launch_stencil(c, kPlain, c->L, c->prec, in, out, nullptr, nullptr, s);  // warm
+        if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
+        float ms = 1e30f;
+        for (int trial = 0; trial < 2; ++trial) {  // best of two trials of five launches
+          cudaEventRecord(e0, s);
+          for (int r = 0; r < 5; ++r) launch_stencil(c, kPlain, c->L, c->prec, in, out, nullptr, nullptr, s);
+          cudaEventRecord(e1, s);
+          cudaEventSynchronize(e1);
+          float t = 0.f;
+          cudaEventElapsedTime(&t, e0, e1);
+          ms = t < ms ? t : ms;
+        }
+        if (ms < best_ms) { best_ms = ms; best = g; }
+      }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   c->sg = best;
@@ -394,14 +436,32 @@ int launch_wait_selftest(int tries, int* flag, cudaStream_t s) {
   return check_launch();
 }
 
+template <int OCC>
+static void set_stencil_smem(int lim) {
+  cudaFuncSetAttribute(k_stencil<float, kPlain, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<float, kPCG, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<double, kPlain, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<double, kPCG, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<double, kResidual, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
+
 int prepare_stencil_kernels() {
-  const int lim = 220 * 1024;  // below the 227 KB opt-in less the static shared memory
-  cudaFuncSetAttribute(k_stencil<float, kPlain>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_stencil<float, kPCG>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_stencil<double, kPlain>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_stencil<double, kPCG>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_stencil<double, kResidual>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  set_stencil_smem<1>(220 * 1024);  // below the 227 KB opt-in less the static shared memory
+  set_stencil_smem<3>(72 * 1024);
   return check_launch();
+}
+
+template <int OCC>
+static void launch_stencil_kernel(int mode, int prec, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                                  const StencilArgs& A) {
+  if (prec == PGJ_FP32) {
+    if (mode == kPlain) k_stencil<float, kPlain, OCC><<<grid, block, smem, s>>>(A);
+    else k_stencil<float, kPCG, OCC><<<grid, block, smem, s>>>(A);
+  } else {
+    if (mode == kPlain) k_stencil<double, kPlain, OCC><<<grid, block, smem, s>>>(A);
+    else if (mode == kPCG) k_stencil<double, kPCG, OCC><<<grid, block, smem, s>>>(A);
+    else k_stencil<double, kResidual, OCC><<<grid, block, smem, s>>>(A);
+  }
 }
 
 int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, void* out, const double* f,
@@ -417,22 +477,15 @@ int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, vo
   // TMA rows need 16-byte aligned starts and sizes: (3 n * element size) % 16 == 0 and an aligned base
   A.tma = ((3 * size_t(n) * tsz) % 16 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0) ? 1 : 0;
   dim3 grid(c->sg.ntiles, c->sg.nchunks, loads), block(n, c->sg.ty + 1);
-  const size_t smem = tsz * (size_t(2) * (c->sg.ty + 2) * 3 * n + size_t(c->sg.ty + 1) * n * 9) + 32 * 4 * 8 + 16 + 64;
+  A.stages = A.tma ? c->sg.stages : 2;
+  const size_t smem = tsz * (size_t(A.stages) * (c->sg.ty + 2) * 3 * n + size_t(c->sg.ty + 1) * n * 9) + 32 * 4 * 8 + 16 +
+                      8 * A.stages + 64;
   if (c->sg.ntiles * c->sg.nchunks > kMaxPartials) return PGJ_ERR_UNSUPPORTED;
-  if (prec == PGJ_FP32) {
-    switch (mode) {
-      case kPlain: k_stencil<float, kPlain><<<grid, block, smem, s>>>(A); break;
-      case kPCG: k_stencil<float, kPCG><<<grid, block, smem, s>>>(A); break;
-      default: return PGJ_ERR_ARGUMENT;
-    }
-  } else {
-    switch (mode) {
-      case kPlain: k_stencil<double, kPlain><<<grid, block, smem, s>>>(A); break;
-      case kPCG: k_stencil<double, kPCG><<<grid, block, smem, s>>>(A); break;
-      case kResidual: k_stencil<double, kResidual><<<grid, block, smem, s>>>(A); break;
-      default: return PGJ_ERR_ARGUMENT;
-    }
-  }
+  if (mode != kPlain && mode != kPCG && !(mode == kResidual && prec == PGJ_FP64)) return PGJ_ERR_ARGUMENT;
+  // the occupancy variant applies to the recurrence operator; the residual keeps the wide form
+  const bool occ3 = c->sg.occ == 3 && mode != kResidual && n * (c->sg.ty + 1) <= 256 && smem <= 72 * 1024;
+  if (occ3) launch_stencil_kernel<3>(mode, prec, grid, block, smem, s, A);
+  else launch_stencil_kernel<1>(mode, prec, grid, block, smem, s, A);
   return check_launch();
 }
 

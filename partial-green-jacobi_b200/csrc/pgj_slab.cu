@@ -13,7 +13,9 @@
 // projection P are exact linear identities moved into the spectral pass:
 //   DFT(s.(r - m)) = DFT(s.r) - m DFT(s),   sum_x s.w = sum_k W(k) conj(DFT(s)(k)).
 // A block owns one component of one z-plane: an n x n real slab, two rows packed per complex
-// line for the real transform, the half spectrum as n rows of nsp (even) complex values.
+// line for the real transform (lines at an odd pitch of n + 1 complex values, so that a warp
+// working on 32 lines at the same index touches distinct banks), the half spectrum as n rows of
+// nsp (even) complex values.
 #include "pgj_fft_engine.cuh"
 #include <cstring>
 
@@ -24,7 +26,7 @@ enum SlabMode { kSlabUpdate = 0, kSlabInit = 1, kSlabSync = 2 };
 struct SlabArgs {
   int n, ns, nsp;
   FFTPlan plan;
-  FastDiv div_n, div_ns;
+  FastDiv div_n, div_ns, div_nh;  // n, ns, n / 2
   void* p;                // (L,3N) T search directions
   const void* q;          // (L,3N) T K p
   void* r;                // (L,3N) T recurrence residual
@@ -70,6 +72,7 @@ __global__ void __launch_bounds__(512, 2) k_fxy(const SlabArgs A) {
   T* r = reinterpret_cast<T*>(A.r) + off;
   const double* sc = A.scale + 3 * node0 + c;
   T* packed = real_view<T>(b0);
+  const int lpx = n + 1;  // pitch of the packed x lines
   double acc[2] = {0.0, 0.0};
   const double alpha = MODE == kSlabUpdate ? S.alpha : 0.0;
   const T a = T(alpha);
@@ -112,19 +115,19 @@ __global__ void __launch_bounds__(512, 2) k_fxy(const SlabArgs A) {
         } else if (MODE == kSlabSync) {
           r[k] = rj;
         }
-        // rows 2l and 2l+1 packed as the real and imaginary parts of complex line l (offset 2 l nsp)
-        packed[2 * ((y >> 1) * 2 * nsp + x) + (y & 1)] = T(sv[j]) * rj;
+        // rows 2l and 2l+1 packed as the real and imaginary parts of complex line l
+        packed[2 * ((y >> 1) * lpx + x) + (y & 1)] = T(sv[j]) * rj;
       }
     }
   }
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_lines<T, false>(b0, b1, n / 2, 2 * nsp, 1, A.plan, A.div_n, tw, false, tid, nthr);
+  C* res = fft_lines<T, true>(b0, b1, n / 2, lpx, 1, A.plan, A.div_nh, tw, false, tid, nthr);
   C* oth = res == b0 ? b1 : b0;
   // split the packed transforms: row rho = 2l (real part) and 2l+1 (imaginary part)
   for (int i = tid; i < n * ns; i += nthr) {
     const int rho = fdiv(i, A.div_ns), k = i - rho * ns;
-    const C* line = res + (rho >> 1) * 2 * nsp;
+    const C* line = res + (rho >> 1) * lpx;
     const C zk = line[k];
     const C zn = line[k == 0 ? 0 : n - k];
     C o;
@@ -204,6 +207,7 @@ __global__ void __launch_bounds__(512, 2) k_ifxy(const SlabArgs A) {
   if (!S.active) return;
   const int n = A.n, ns = A.ns, nsp = A.nsp;
   const int nn = n * n;
+  const int lpx = n + 1;  // pitch of the packed x lines
   C* b0 = reinterpret_cast<C*>(smem_raw);
   C* b1 = b0 + size_t(n) * nsp;
   const C* sp = reinterpret_cast<const C*>(A.spec) + ((size_t(load) * 3 + c) * n + z) * size_t(n) * nsp;
@@ -238,10 +242,10 @@ __global__ void __launch_bounds__(512, 2) k_ifxy(const SlabArgs A) {
     C zz;
     zz.x = v[0].x - v[1].y;
     zz.y = v[0].y + v[1].x;
-    oth[l * 2 * nsp + k] = zz;
+    oth[l * lpx + k] = zz;
   }
   __syncthreads();
-  C* res2 = fft_lines<T, false>(oth, res, n / 2, 2 * nsp, 1, A.plan, A.div_n, tw, true, tid, nthr);
+  C* res2 = fft_lines<T, true>(oth, res, n / 2, lpx, 1, A.plan, A.div_nh, tw, true, tid, nthr);
   const T* wv = real_view<T>(res2);
   const size_t node0 = size_t(z) * nn;
   const size_t off = size_t(load) * 3 * size_t(nn) * n + 3 * node0 + c;
@@ -267,7 +271,7 @@ __global__ void __launch_bounds__(512, 2) k_ifxy(const SlabArgs A) {
       const int i = i0 + j * nthr;
       if (i < nn) {
         const int y = fdiv(i, A.div_n), x = i - y * n;
-        const T w = wv[2 * ((y >> 1) * 2 * nsp + x) + (y & 1)];
+        const T w = wv[2 * ((y >> 1) * lpx + x) + (y & 1)];
         const T zv = T(sv[j]) * w - m;
         p[3 * size_t(i)] = A.init ? zv : zv + beta * pv[j];
       }
@@ -315,6 +319,7 @@ static SlabArgs slab_args(pgj_ctx* c, int loads, int prec) {
   A.plan = c->plan;
   A.div_n = make_fastdiv(unsigned(c->n));
   A.div_ns = make_fastdiv(unsigned(c->ns));
+  A.div_nh = make_fastdiv(unsigned(c->n / 2));
   A.p = c->p; A.q = c->q; A.r = c->r;
   A.r64 = c->r64; A.scale = c->scale; A.spec = c->spec;
   A.tw = prec == PGJ_FP32 ? static_cast<const void*>(static_cast<double2*>(c->tw) + c->n) : c->tw;

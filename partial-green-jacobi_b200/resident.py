@@ -224,6 +224,13 @@ class Operator:
             names = ["operator", "update_ur", "fft_x", "fft_y", "fft_z_symbol", "ifft_y", "ifft_x", "update_p"]
         return {k: dict(ms=ms[i], bytes=nbytes[i]) for i, k in enumerate(names)}
 
+    def tile_shapes(self) -> dict:
+        """Tile shapes picked by the operator and Green-pass autotuners for this context."""
+        out = (C.c_int * 6)()
+        _lib.check(_lib.lib().pgj_tile_shapes(self._ctx, out), "pgj_tile_shapes")
+        return dict(stencil_rows=out[0], stencil_planes=out[1], fft_rows=out[2], fft_y_columns=out[3],
+                    fft_z_columns=out[4], fused=bool(out[5]))
+
     @property
     def fused_iteration(self) -> bool:
         """True when one PCG iteration runs as four kernels (slab-fused updates and transforms)."""
