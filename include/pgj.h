@@ -197,7 +197,10 @@ int pgj_cone_filter(int n, const int32_t* offsets, const double* weights, int co
 int pgj_paper_project(int n, const double* t, const double* hs, double beta, double eta, double emin,
                       double* ph, double* dp, double* a, void* stream);
 /* Full OC update: inputs x, ph, dp, hs, local objective density `energy`; output `xnew` and
- * host `steps` (bisections taken) and `change` (max |xnew - x|). scratch: 4 n^3 float64 device. */
+ * host `steps` (bisections taken) and `change` (max |xnew - x|), read back with one stream
+ * synchronisation. With steps and change both NULL the update is only enqueued (no
+ * synchronisation); the bisections taken and the change are then left at scratch[4 n^3 + 3] and
+ * scratch[4 n^3 + 4]. scratch: 4 n^3 + 512 float64 device. */
 int pgj_paper_oc(int n, const int32_t* offsets, const double* weights, int count, const double* x,
                  const double* ph, const double* dp, const double* hs, const double* energy,
                  double volume, double beta, double eta, double emin, double move, double exponent,

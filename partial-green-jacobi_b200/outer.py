@@ -139,5 +139,20 @@ class PaperOuter:
                    "pgj_paper_oc")
         self.steps, self.change = steps.value, ch.value
 
+    def step_async(self, e):
+        """OC update enqueued on the current stream without a host synchronisation; ``record()``
+        reads (steps, change) afterwards from the device scratch."""
+        if e.data_ptr() != self.energy.data_ptr():
+            self.energy.copy_(e)
+        _lib.check(_lib.lib().pgj_paper_oc(self.n, _p(self.offsets), _p(self.weights), self.weights.numel(), _p(self.x),
+                                           _p(self.ph), _p(self.dp), _p(self.hs), _p(self.energy), self.volume,
+                                           self.beta, self.eta, self.emin, self.move, self.exponent, self.floor,
+                                           _p(self.new), _p(self.scratch), None, None, _sp()), "pgj_paper_oc")
+
+    def record(self):
+        """Device view of (steps, change) of the last asynchronous OC update."""
+        N = self.n ** 3
+        return self.scratch[4 * N + 3:4 * N + 5]
+
     def advance(self):
         self.x.copy_(self.new)

@@ -471,3 +471,61 @@ def test_design_step_objective_and_sensitivity(pkg, oracle):
     assert rel(local.cpu().numpy().ravel(), local_ref) < 1e-8
     assert abs(float(f) - (local_ref * a.ravel()).mean()) < 1e-11
     assert rel(diag.cpu().numpy(), (e * a.reshape(1, -1)).mean(1)) < 1e-8
+
+
+def test_serving_design_steps_same_alone_and_in_mix(pkg):
+    """Continuous batching: a lineage's design steps give the same results alone and among other
+    lineages and homogenizations of other grid sizes that overlap it on the device."""
+    sv = pkg.serve
+    lin = sv.Lineage(n=16, seed=3, emin=1e-4, steps=3, tag="L")
+    hom = sv.Homogenize(pkg.baseline_design(16, 5, 1e-6), 0.5, tag="H")
+    alone = sv.Server(precision="mixed").run([sv.Arrival(0.0, lin), sv.Arrival(0.0, hom)], realtime=False)
+    mix = [sv.Arrival(0.0, lin), sv.Arrival(0.0, hom)]
+    mix += [sv.Arrival(0.0, sv.Lineage(n=m, seed=10 + k, emin=1e-6, steps=2, tag=k)) for k, m in enumerate((12, 20, 24))]
+    server = sv.Server(precision="mixed", max_workers_per_n=2)
+    got = server.run(mix, realtime=False)
+    assert server.max_inflight >= 2
+    assert all(r.status == 0 for r in got + alone)
+    assert len([r for r in got if r.kind == "design_step"]) == 3 + 3 * 2
+    for tag, steps in (("L", 3), ("H", 1)):
+        for step in range(steps):
+            a = [r for r in alone if r.tag == tag and r.step == step][0]
+            b = [r for r in got if r.tag == tag and r.step == step][0]
+            assert rel(b.C, a.C) <= 1e-12, (tag, step, rel(b.C, a.C))
+            if tag == "L":
+                assert b.objective == pytest.approx(a.objective, rel=1e-12)
+                assert b.oc_steps == a.oc_steps and b.oc_steps > 0
+    # the homogenization request equals a direct certified solve of the same field
+    lam, mu = pkg.PAPER_MEDIUM
+    op = pkg.Operator(16, 6, lam, mu, precision="mixed")
+    op.set_material(dev(pkg.baseline_design(16, 5, 1e-6)))
+    op.set_alpha(0.5)
+    u = torch.zeros((6, 3 * 16 ** 3), dtype=torch.float64, device="cuda")
+    _, st = op.solve(np.eye(6), 1e-8, u)
+    assert st == 0
+    C = op.effective_tensor(u).cpu().numpy()
+    h = [r for r in got if r.tag == "H"][0]
+    assert rel(h.C, C) <= 1e-12
+
+
+def test_serving_design_step_matches_oracle_chain(pkg, oracle):
+    """First design step of a lineage: filter/projection, certified solve, shear objective and OC
+    update against the CPU restatement."""
+    sv = pkg.serve
+    n = 10
+    lin = sv.Lineage(n=n, seed=4, emin=1e-4, steps=1, volume=0.3, rmin=1.5, move=0.2, tag=0)
+    res = sv.Server(precision="fp64").run([sv.Arrival(0.0, lin)], realtime=False)
+    assert len(res) == 1 and res[0].status == 0
+    lam, mu = pkg.PAPER_MEDIUM
+    x0 = pkg.baseline_density(n, 4, 0.3)
+    t = oracle.cone_filter(x0, 1.5)
+    hs = oracle.cone_filter(np.ones_like(x0), 1.5)
+    ph, dp, a = oracle.paper_physical(t, hs, 4.0, 0.5, 1e-4)
+    ref = oracle.homogenize(a, lam, mu, 0.5)
+    assert rel(res[0].C, ref["C"]) < 1e-10
+    e = oracle.energies(ref["u"], oracle.affine(n, np.eye(6)), n, lam, mu)
+    local = -e[3:].sum(0)
+    assert res[0].objective == pytest.approx((local * a.reshape(-1)).mean(), rel=1e-9)
+    _, steps, change = oracle.paper_oc(x0, local.reshape(x0.shape), ph, dp, hs, 1.5, 0.3, 4.0, 0.5, 1e-4, move=0.2)
+    assert res[0].oc_steps == steps
+    assert res[0].change == pytest.approx(change, rel=1e-6, abs=1e-9)
