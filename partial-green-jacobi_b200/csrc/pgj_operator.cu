@@ -159,21 +159,23 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   }
   const T* in = reinterpret_cast<const T*>(A.in) + size_t(load) * 3 * N;
 
-  // plane j (node plane z0 - 1 + j) sits in buffer j % NS; TMA staging keeps NS - 1 planes in flight,
-  // the cp.async fallback two
+  // plane j (node plane z0 - 1 + j) sits in buffer j % NS; with TMA staging every buffer is refilled
+  // as soon as the block barrier after its last read has passed, so NS - 1 planes stay in flight
   const int NS = A.tma ? A.stages : 2;
   const int planevals = (TY + 2) * 3 * n;
+  const int nt = n * (TY + 1);
   T* bufs = reinterpret_cast<T*>(smem_raw);
-  T* upy = bufs + NS * planevals;          // (TY+1) * n * 6
-  T* upx = upy + (TY + 1) * n * 6;         // (TY+1) * n * 3
-  double* red = reinterpret_cast<double*>(upx + (TY + 1) * n * 3 + 2);  // 32 * 4, 16-byte padded
+  // corner exchange, double-buffered by step parity: [parity][corner 10 / 01 / 11][thread][3]
+  T* xch = bufs + NS * planevals;
+  const int xsz = 3 * nt * 3;
+  double* red = reinterpret_cast<double*>(xch + 2 * xsz + 2);  // 32 * 4, 16-byte padded
   red = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(red) + 15) & ~uintptr_t(15));
   uint64_t* bars = reinterpret_cast<uint64_t*>(red + 32 * 4);  // NS mbarriers (TMA staging)
   const bool tma = A.tma != 0;
   const int nplanes = zc + 2;
-  T* buf0 = bufs;
 
-  // prologue: planes j = 0 .. NS-1 (plane 0 is z0 - 1)
+  // prologue: planes j = 0 .. NS-1 (plane 0 is z0 - 1); plane 0 gives the first lower face
+  bool bad = false;
   if (tma) {
     if (tid == 0) {
       for (int b = 0; b < NS; ++b) mbar_init(&bars[b], 1);
@@ -183,11 +185,7 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
     if (tid == 0)
       for (int j = 0; j < NS && j < nplanes; ++j)
         tma_plane(bufs + j * planevals, in, (z0 - 1 + j + n) % n, y0, TY + 2, n, &bars[j]);
-    const bool okw = tid == 0 ? mbar_wait(&bars[0], 0) : true;
-    if (__syncthreads_or(!okw)) {
-      if (tid == 0 && A.err) atomicExch(A.err, 1);
-      return;
-    }
+    bad = !mbar_wait(&bars[0], 0);  // every thread observes the arrival (acquire)
   } else {
     stage_plane(bufs, in, (z0 - 1 + n) % n, y0, TY + 2, n, tid, nthr);
     stage_plane(bufs + planevals, in, z0 % n, y0, TY + 2, n, tid, nthr);
@@ -195,7 +193,15 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
     __syncthreads();
   }
   T F0[4][3], own[3], dummy[3];
-  face_modes(buf0, ty, tx, n, F0, dummy);
+  face_modes(bufs, ty, tx, n, F0, dummy);
+  if (tma) {
+    // buffer 0 is free once every thread has read plane 0
+    if (__syncthreads_or(bad)) {
+      if (tid == 0 && A.err) atomicExch(A.err, 1);
+      return;
+    }
+    if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0]);
+  }
   T Up[4][3];
 #pragma unroll
   for (int f = 0; f < 4; ++f)
@@ -213,10 +219,14 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   int za = (z0 - 1 + n) % n;  // element plane of the next density read (wraps incrementally)
   double a_next = __ldg(arow + size_t(za) * aplane);
   // buffer / phase bookkeeping without divisions: plane j = s + 1 sits in buffer jb with mbarrier
-  // parity jpar; plane s (refilled with plane s + NS) in buffer sb; zr = node plane s + NS (mod n)
-  int jb = 1 % NS, sb = 0;
+  // parity jpar; after the step's barrier that buffer takes plane s + 1 + NS (node plane zr)
+  int jb = 1 % NS;
   unsigned jpar = 0u;
-  int zr = (z0 - 1 + NS) % n;
+  int zr = (z0 + NS) % n;
+  const int tl = ty * n + (tx == 0 ? n - 1 : tx - 1);          // element to the left (periodic x)
+  const int tb = (ty >= 1 ? ty - 1 : 0) * n + tx;              // element below
+  const int tbl = (ty >= 1 ? ty - 1 : 0) * n + (tx == 0 ? n - 1 : tx - 1);
+  const int tme = ty * n + tx;
   for (int s = 0; s <= zc; ++s) {
     const int ez = z0 - 1 + s;           // element plane
     const T ae = T(a_next);
@@ -226,22 +236,12 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
     }
     T* cur = bufs + jb * planevals;
     if (tma) {
-      // one thread observes the plane's arrival (acquire); the block barrier publishes it
-      const bool okw = tid == 0 ? mbar_wait(&bars[jb], jpar) : true;
-      if (__syncthreads_or(!okw)) {
-        if (tid == 0 && A.err) atomicExch(A.err, 1);
-        return;
-      }
-      // plane s was consumed by the previous step: refill its buffer with plane s + NS
-      if (tid == 0 && s + NS < nplanes) tma_plane(bufs + sb * planevals, in, zr, y0, TY + 2, n, &bars[sb]);
+      bad = bad || !mbar_wait(&bars[jb], jpar);
     } else {
       cp_wait_all();
       __syncthreads();
       if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
     }
-    if (++jb == NS) { jb = 0; jpar ^= 1u; }
-    sb = sb + 1 == NS ? 0 : sb + 1;
-    zr = zr + 1 == n ? 0 : zr + 1;
 
     T F1[4][3], own1[3];
     face_modes(cur, ty, tx, n, F1, own1);
@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
       }
     T P[8][3];
     element_modal<T>(Q, ae, A.kc, P);
-    // z-level transpose: U -> upper plane (ez+1), D -> lower plane (ez)
+    // z-level transpose: U -> upper plane (ez+1), G -> lower plane (ez)
     T U[4][3], G[4][3];
 #pragma unroll
     for (int f = 0; f < 4; ++f)
@@ -265,52 +265,51 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
         U[f][c] = P[f][c] + P[f + 4][c];
         G[f][c] = (P[f][c] - P[f + 4][c]) + Up[f][c];
       }
+    // lower face of the element (node plane ez) as its four corner nodes: this thread keeps the
+    // (x, y) corner and hands (x+1, y), (x, y+1), (x+1, y+1) to their owners through shared memory
+    T c00[3];
+    T* xb = xch + (s & 1) * xsz;
     if (s >= 1) {
-      // output plane ez: y level
-      T R[2][3];
 #pragma unroll
-      for (int mx = 0; mx < 2; ++mx)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          upy[(ty * n + tx) * 6 + mx * 3 + c] = G[mx][c] + G[mx + 2][c];
-          R[mx][c] = G[mx][c] - G[mx + 2][c];
-        }
-      __syncthreads();
-      T qx[3];
-      if (ty >= 1) {
-#pragma unroll
-        for (int mx = 0; mx < 2; ++mx)
-#pragma unroll
-          for (int c = 0; c < 3; ++c) R[mx][c] += upy[((ty - 1) * n + tx) * 6 + mx * 3 + c];
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          upx[(ty * n + tx) * 3 + c] = R[0][c] + R[1][c];
-          qx[c] = R[0][c] - R[1][c];
-        }
+      for (int c = 0; c < 3; ++c) {
+        const T ly0 = G[0][c] - G[2][c], ly1 = G[1][c] - G[3][c];
+        const T uy0 = G[0][c] + G[2][c], uy1 = G[1][c] + G[3][c];
+        c00[c] = ly0 - ly1;
+        xb[(0 * nt + tme) * 3 + c] = ly0 + ly1;
+        xb[(1 * nt + tme) * 3 + c] = uy0 - uy1;
+        xb[(2 * nt + tme) * 3 + c] = uy0 + uy1;
       }
-      __syncthreads();
-      if (out_row) {
-        const int xm = tx == 0 ? n - 1 : tx - 1;
+    }
+    // one barrier per step: corners published, plane jb fully read, timeouts agreed on
+    if (__syncthreads_or(bad)) {
+      if (tid == 0 && A.err) atomicExch(A.err, 1);
+      return;
+    }
+    if (tma && tid == 0 && s + 1 + NS < nplanes) tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb]);
+    if (++jb == NS) { jb = 0; jpar ^= 1u; }
+    zr = zr + 1 == n ? 0 : zr + 1;
+    if (s >= 1 && out_row) {
+      T qx[3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) qx[c] += upx[(ty * n + xm) * 3 + c];
-        const size_t node = (size_t(ez) * n + ey) * n + tx;
-        T* o = out + 3 * node;
-        if (MODE == kResidual) {
-          const double* fl = A.f + size_t(load) * 3 * N + 3 * node;
+      for (int c = 0; c < 3; ++c)
+        qx[c] = ((c00[c] + xb[(0 * nt + tl) * 3 + c]) + xb[(1 * nt + tb) * 3 + c]) + xb[(2 * nt + tbl) * 3 + c];
+      const size_t node = (size_t(ez) * n + ey) * n + tx;
+      T* o = out + 3 * node;
+      if (MODE == kResidual) {
+        const double* fl = A.f + size_t(load) * 3 * N + 3 * node;
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            const double rv = fl[c] - double(qx[c]);
-            o[c] = T(rv);
-            acc[0] += rv * rv;
-            acc[1 + c] += rv;
-          }
-        } else {
+        for (int c = 0; c < 3; ++c) {
+          const double rv = fl[c] - double(qx[c]);
+          o[c] = T(rv);
+          acc[0] += rv * rv;
+          acc[1 + c] += rv;
+        }
+      } else {
 #pragma unroll
-          for (int c = 0; c < 3; ++c) o[c] = qx[c];
-          if (MODE == kPCG) {
+        for (int c = 0; c < 3; ++c) o[c] = qx[c];
+        if (MODE == kPCG) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) acc[0] += double(own[c]) * double(qx[c]);
-          }
+          for (int c = 0; c < 3; ++c) acc[0] += double(own[c]) * double(qx[c]);
         }
       }
     }
@@ -478,8 +477,8 @@ int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, vo
   A.tma = ((3 * size_t(n) * tsz) % 16 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0) ? 1 : 0;
   dim3 grid(c->sg.ntiles, c->sg.nchunks, loads), block(n, c->sg.ty + 1);
   A.stages = A.tma ? c->sg.stages : 2;
-  const size_t smem = tsz * (size_t(A.stages) * (c->sg.ty + 2) * 3 * n + size_t(c->sg.ty + 1) * n * 9) + 32 * 4 * 8 + 16 +
-                      8 * A.stages + 64;
+  const size_t smem = tsz * (size_t(A.stages) * (c->sg.ty + 2) * 3 * n + size_t(2) * 9 * (c->sg.ty + 1) * n) +
+                      32 * 4 * 8 + 16 + 8 * A.stages + 64;
   if (c->sg.ntiles * c->sg.nchunks > kMaxPartials) return PGJ_ERR_UNSUPPORTED;
   if (mode != kPlain && mode != kPCG && !(mode == kResidual && prec == PGJ_FP64)) return PGJ_ERR_ARGUMENT;
   // the occupancy variant applies to the recurrence operator; the residual keeps the wide form

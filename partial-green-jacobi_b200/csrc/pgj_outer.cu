@@ -330,7 +330,7 @@ int pgj_study1_oc(int n, const double* weights, int radius, const double* x, con
   // the candidate of the last bisection is the returned design (study.py:91-100)
   k_absmax_diff<<<1, 1024, 0, s>>>(N, xnew, x, w.bounds + 4);
   if ((st = check_launch())) return st;
-  if (!steps && !change) return PGJ_OK;  // enqueue only: the record stays in scratch[4N + 3 .. 4N + 4]
+  if (!change) return PGJ_OK;  // enqueue only: the change stays in scratch[4N + 4]
   double host[8];
   e = cudaMemcpyAsync(host, w.bounds, sizeof(host), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
