@@ -19,6 +19,12 @@ free up, so their work overlaps on the device (continuous batching, not a queue 
 solver). Every step is issued asynchronously; the loop polls CUDA events and never waits for one
 request while others could be admitted. Results are identical whether a request runs alone or in a
 mix: each context is private to one request at a time and every kernel reduces in a fixed order.
+
+Precision. A mixed server runs FP32 inner recurrences (FP64 certificate) where they pay: lineages
+whose Emin is below ``fp64_below_emin`` (a contrast the FP32 operator no longer resolves, so the
+FP32 recurrence stalls near the target) run in FP64 from the start, and any mixed request that fails
+certification is redone in FP64, warm-started from the mixed iterate. A design step commits its OC
+update only once its solve is certified.
 """
 from __future__ import annotations
 
@@ -104,12 +110,14 @@ class StepResult:
     device_ms: float     # first to last device operation of the step (CUDA events)
     oc_steps: int = 0
     change: float = 0.0
+    precision: str = ""  # "mixed", "fp64", or "fp64-fallback" (redone after a mixed failure)
 
 
 class _Worker:
     def __init__(self, n: int, precision: str, lam: float, mu: float):
         torch = _torch()
         self.n = n
+        self.precision = precision
         self.stream = torch.cuda.Stream()
         with torch.cuda.stream(self.stream):
             self.op = Operator(n, 6, lam, mu, precision)
@@ -133,6 +141,7 @@ class _LineageState:
         self.u = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")  # warm start
         self.step = 0
         self.bytes = lineage_bytes(n)
+        self.pending_advance = False  # the last certified step's OC update waits to be committed
 
 
 @dataclass
@@ -144,6 +153,9 @@ class _Job:
     admitted: float = 0.0
     start: object = None
     end: object = None
+    precision: str = "fp64"
+    fallback: bool = False           # FP64 redo of a mixed request that failed certification
+    u_start: object = None           # homogenization redo: the mixed iterate as the FP64 warm start
 
 
 def worker_bytes(n: int, precision: str) -> int:
@@ -165,8 +177,11 @@ class Server:
     """Continuous batching over libpgj contexts under an HBM budget (bytes)."""
 
     def __init__(self, precision: str = "mixed", hbm_budget: float = 120e9, max_workers_per_n: int = 4,
-                 rtol: float = 1e-8, medium=PAPER_MEDIUM):
+                 rtol: float = 1e-8, medium=PAPER_MEDIUM, fp64_below_emin: float = 1e-7, fallback: bool = True):
         self.precision = precision
+        self.fp64_below_emin = float(fp64_below_emin)
+        self.fallback = bool(fallback)
+        self.fallbacks = 0     # mixed requests redone in FP64
         self.budget = int(hbm_budget)
         self.max_workers_per_n = int(max_workers_per_n)
         self.rtol = float(rtol)
@@ -184,22 +199,28 @@ class Server:
     def _need(self, job: _Job) -> int:
         return lineage_bytes(job.req.n) if isinstance(job.req, Lineage) and job.lineage is None else 0
 
-    def _worker_for(self, n: int, extra: int) -> _Worker | None:
-        free = [w for w in self.workers if w.n == n and w.job is None]
+    def _precision_for(self, req) -> str:
+        if self.precision == "mixed" and isinstance(req, Lineage) and req.emin < self.fp64_below_emin:
+            return "fp64"
+        return self.precision
+
+    def _worker_for(self, n: int, prec: str, extra: int) -> _Worker | None:
+        free = [w for w in self.workers if w.n == n and w.precision == prec and w.job is None]
         if free:
             return free[0] if self.used + extra <= self.budget else None
-        if sum(1 for w in self.workers if w.n == n) >= self.max_workers_per_n:
+        if sum(1 for w in self.workers if w.n == n and w.precision == prec) >= self.max_workers_per_n:
             return None
-        need = worker_bytes(n, self.precision) + extra
-        # evict idle workers of other grid sizes, least recently used first, while over budget
-        idle = sorted((w for w in self.workers if w.job is None and w.n != n), key=lambda w: w.last_used)
+        need = worker_bytes(n, prec) + extra
+        # evict idle workers of other kinds, least recently used first, while over budget
+        idle = sorted((w for w in self.workers if w.job is None and (w.n != n or w.precision != prec)),
+                      key=lambda w: w.last_used)
         while self.used + need > self.budget and idle:
             w = idle.pop(0)
             self.workers.remove(w)
             self.used -= w.bytes
         if self.used + need > self.budget:
             return None
-        w = _Worker(n, self.precision, self.lam, self.mu)
+        w = _Worker(n, prec, self.lam, self.mu)
         self.workers.append(w)
         self.used += w.bytes
         return w
@@ -218,6 +239,9 @@ class Server:
                     job.lineage = _LineageState(job.req)
                     self.used += job.lineage.bytes
                 ls = job.lineage
+                if ls.pending_advance:                  # commit the previous certified step's update
+                    ls.outer.advance()
+                    ls.pending_advance = False
                 ls.outer.evaluate()                     # filter + projection + SIMP -> outer.a
                 w.op.set_material(ls.outer.a)
                 w.op.set_alpha(job.req.alpha)
@@ -227,7 +251,10 @@ class Server:
                 a = a.to("cuda", non_blocking=True) if not a.is_cuda else a
                 w.op.set_material(a.contiguous())
                 w.op.set_alpha(job.req.alpha)
-                w.u0.zero_()
+                if job.u_start is not None:
+                    w.u0.copy_(job.u_start)             # the mixed iterate
+                else:
+                    w.u0.zero_()
                 u = w.u0
             _lib.check(L.pgj_solve_async(w.op._ctx, 6, self.macros.ctypes.data, self.rtol, u.data_ptr(),
                                          w.stream.cuda_stream), "pgj_solve_async")
@@ -241,8 +268,7 @@ class Server:
                 w.scal[0] = (local * ls.outer.a.reshape(-1)).mean()
                 ls.outer.step_async(local.reshape(ls.outer.x.shape))
                 w.scal[1:3].copy_(ls.outer.record())
-                ls.outer.advance()
-                w.sh.copy_(w.scal, non_blocking=True)
+                w.sh.copy_(w.scal, non_blocking=True)   # x <- new waits for the certificate
             job.end = torch.cuda.Event(enable_timing=True)
             job.end.record(w.stream)
 
@@ -259,7 +285,8 @@ class Server:
                          objective=float(w.sh[0]) if lineage else float("nan"), status=st, iterations=its,
                          queued_ms=(job.admitted - job.ready) * 1e3, latency_ms=(now - job.ready) * 1e3,
                          device_ms=job.start.elapsed_time(job.end),
-                         oc_steps=int(w.sh[1]) if lineage else 0, change=float(w.sh[2]) if lineage else 0.0)
+                         oc_steps=int(w.sh[1]) if lineage else 0, change=float(w.sh[2]) if lineage else 0.0,
+                         precision="fp64-fallback" if job.fallback else w.precision)
         w.job = None
         w.last_used = now
         return res
@@ -280,13 +307,14 @@ class Server:
                 req = arr.req
                 if isinstance(req, Lineage) and not supported_n(req.n):
                     raise ValueError(f"unsupported grid size {req.n}")
-                ready.append(_Job(req=req, ready=t0 + arr.t if realtime else now))
+                ready.append(_Job(req=req, ready=t0 + arr.t if realtime else now,
+                                  precision=self._precision_for(req)))
             progressed = False
             # admission in arrival order; a request that cannot start does not block other sizes
             still: deque[_Job] = deque()
             while ready:
                 job = ready.popleft()
-                w = self._worker_for(self._n_of(job.req), self._need(job))
+                w = self._worker_for(self._n_of(job.req), job.precision, self._need(job))
                 if w is None:
                     still.append(job)
                     continue
@@ -297,7 +325,7 @@ class Server:
             ready = still
             if ready and not inflight and not any(w.job for w in self.workers):
                 job = ready[0]
-                need = worker_bytes(self._n_of(job.req), self.precision) + self._need(job)
+                need = worker_bytes(self._n_of(job.req), job.precision) + self._need(job)
                 if need > self.budget:
                     raise RuntimeError(f"request needs {need} bytes, more than the HBM budget {self.budget}")
             self.max_inflight = max(self.max_inflight, len(inflight))
@@ -306,13 +334,27 @@ class Server:
                 if w.job.end.query():
                     now = time.perf_counter()
                     job = w.job
-                    results.append(self._finish(w, now))
+                    res = self._finish(w, now)
                     inflight.remove(w)
                     progressed = True
+                    if res.status != 0 and job.precision == "mixed" and self.fallback:
+                        # redo in FP64 from the mixed iterate; the design does not advance
+                        self.fallbacks += 1
+                        redo = _Job(req=job.req, ready=job.ready, lineage=job.lineage, step=job.step,
+                                    precision="fp64", fallback=True)
+                        if job.lineage is None:
+                            redo.u_start = w.u0.clone()
+                            torch.cuda.current_stream().synchronize()  # copy done before the redo's stream
+                        ready.appendleft(redo)
+                        continue
+                    results.append(res)
                     if job.lineage is not None:
+                        if res.status == 0:
+                            job.lineage.pending_advance = True
                         job.lineage.step += 1
                         if job.lineage.step < job.req.steps:
-                            ready.append(_Job(req=job.req, ready=now, lineage=job.lineage, step=job.lineage.step))
+                            ready.append(_Job(req=job.req, ready=now, lineage=job.lineage, step=job.lineage.step,
+                                              precision=job.precision))
                         else:
                             self.used -= job.lineage.bytes
             if not progressed:

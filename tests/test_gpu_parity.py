@@ -529,3 +529,19 @@ def test_serving_design_step_matches_oracle_chain(pkg, oracle):
     _, steps, change = oracle.paper_oc(x0, local.reshape(x0.shape), ph, dp, hs, 1.5, 0.3, 4.0, 0.5, 1e-4, move=0.2)
     assert res[0].oc_steps == steps
     assert res[0].change == pytest.approx(change, rel=1e-6, abs=1e-9)
+
+
+def test_serving_mixed_falls_back_to_fp64_and_certifies(pkg):
+    """High-contrast lineages run FP64 by policy; a mixed request that fails certification is
+    redone in FP64 from the mixed iterate, and the result is certified."""
+    sv = pkg.serve
+    lin = sv.Lineage(n=24, seed=8, emin=1e-9, steps=2, tag="hi")
+    res = sv.Server(precision="mixed").run([sv.Arrival(0.0, lin)], realtime=False)
+    assert [r.precision for r in res] == ["fp64", "fp64"] and all(r.status == 0 for r in res)
+    # forced onto the mixed path, this n=54, Emin=1e-9 design stalls near 2e-8 at the iteration cap
+    # (FP32 operator error amplified by the contrast); the FP64 redo certifies
+    server = sv.Server(precision="mixed", fp64_below_emin=0.0)
+    lin = sv.Lineage(n=54, seed=1004, emin=1e-9, steps=1, tag="forced")
+    out = server.run([sv.Arrival(0.0, lin)], realtime=False)
+    assert len(out) == 1 and server.fallbacks == 1
+    assert out[0].precision == "fp64-fallback" and out[0].status == 0
