@@ -14,6 +14,11 @@ Green-Jacobi alpha=0.5, every load certified to relative true residual <= 1e-8, 
 * roofline     dominant kernel of the PCG iteration, timed live with CUDA events (pgj_profile_iteration).
 * cpu_baseline the CPU restatement of the reference arithmetic (oracle/pgj_oracle.py) on a
                bounded sample, extrapolated to one homogenization.
+* serving      continuous batching (pgj_b200.serve): Poisson arrivals of design lineages with n
+               log-uniform over [16, 96] and Emin in {1e-4, 1e-6, 1e-9}; each design step is a
+               warm-started certified homogenization, the shear sensitivity and the OC update
+               (move 0.2, filter radius 1.5) on the device; throughput and p50/p99 step latency on
+               the host clock, mixed and plain FP64 servers on the same arrivals.
 Multi-GPU: replicas only (independent designs per rank, no collective on the data path); the
 timing is max-over-ranks; value = all homogenizations / that time.
 """
@@ -114,11 +119,12 @@ class ClockSampler:
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def traffic_from_profiles(kernel):
+def traffic_from_profiles(kernel, prec):
+    """DRAM bytes per launch (ncu dram__bytes_read.sum + dram__bytes_write.sum) of `kernel` at n=64."""
     p = ROOT / "profiles" / "traffic_n64.json"
     if p.exists():
         d = json.loads(p.read_text())
-        return d.get(kernel)
+        return d.get(prec, {}).get(kernel)
     return None
 
 
@@ -215,7 +221,7 @@ def run_gpu(args, rank, world, local_rank):
             torch.cuda.synchronize()
             Cs[prec] = [C.cpu().numpy() for C in tensors]
             out[prec] = dict(total_ms=total_ms, lat=lat, iters=iters, launches=launches, prof=prof,
-                             clocks=clocks.summary(), sweeps=sweeps)
+                             clocks=clocks.summary(), sweeps=sweeps, tiles=op.tile_shapes())
             del op
         # C_H of the mixed path against the FP64 path on the same designs
         errs = [float(np.abs(a - b).max() / np.abs(b).max()) for a, b in zip(Cs["mixed"], Cs["fp64"])]
@@ -274,14 +280,46 @@ def run_gpu(args, rank, world, local_rank):
     out["e2e_ms"] = e2e_ms
     out["h2d"] = host[0].nbytes
     out["d2h"] = 36 * 8
+    if args.serve_lineages > 0 and rank == 0:
+        out["serving"] = run_serving(args, pkg)
     return out
 
 
-def roofline(prof, hbm, kind):
+def run_serving(args, pkg):
+    """Continuous batching of design lineages, mixed and plain FP64 servers on the same arrivals."""
+    sv = pkg.serve
+    arrivals = sv.poisson_lineages(args.serve_lineages, args.serve_rate, seed=11, steps=args.serve_steps)
+    out = {"config": {"lineages": args.serve_lineages, "steps_per_lineage": args.serve_steps,
+                      "arrival_rate_per_s": args.serve_rate, "n": [a.req.n for a in arrivals],
+                      "emin": [a.req.emin for a in arrivals], "hbm_budget_gb": 120, "move": 0.2, "rmin": 1.5,
+                      "volume": 0.3, "alpha": ALPHA, "objective": "shear",
+                      "mixed_policy": "FP64 for Emin < 1e-7; FP64 redo of mixed steps that fail certification",
+                      "latency": "host clock, step ready -> C_H and OC record on the host (queueing included)"}}
+    for prec in ("mixed", "fp64"):
+        # contexts of every grid size once first, so the tile autotuners stay outside the timed run
+        for n in sorted({a.req.n for a in arrivals}):
+            for p in {prec, "fp64"}:
+                pkg.Operator(n, 6, *pkg.PAPER_MEDIUM, precision=p)
+        server = sv.Server(precision=prec, hbm_budget=120e9)
+        t0 = time.perf_counter()
+        res = server.run(arrivals, realtime=True)
+        wall = time.perf_counter() - t0
+        s = sv.summarize(res, wall)
+        s.update(max_in_flight=server.max_inflight, peak_hbm_gb=server.peak_used / 1e9,
+                 iterations_mean=float(np.mean([r.iterations for r in res])), fallbacks=server.fallbacks,
+                 steps_by_precision={k: sum(1 for r in res if r.precision == k)
+                                     for k in sorted({r.precision for r in res})})
+        out[prec] = s
+    out["over_plain_fp64"] = out["mixed"]["homogenizations_per_s"] / out["fp64"]["homogenizations_per_s"]
+    return out
+
+
+def roofline(prof, hbm, kind, prec):
     dom = max(prof, key=lambda k: prof[k]["ms"])
     achieved = prof[dom]["bytes"] / (prof[dom]["ms"] * 1e-3) / 1e9
     return {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-            "frac": achieved / hbm, "peak_kind": kind, "traffic": traffic_from_profiles(dom),
+            "frac": achieved / hbm, "peak_kind": kind, "algorithmic_bytes": prof[dom]["bytes"],
+            "traffic": traffic_from_profiles(dom, prec),
             "iteration_ms": sum(v["ms"] for v in prof.values()),
             "kernels": {k: {"ms": v["ms"], "GBps": v["bytes"] / (v["ms"] * 1e-3) / 1e9} for k, v in prof.items()}}
 
@@ -294,6 +332,9 @@ def main():
     ap.add_argument("--impl", choices=["pgj", "reference"], default="pgj")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--slots", type=int, default=4, help="designs in flight in the batched path")
+    ap.add_argument("--serve-lineages", type=int, default=6, help="design lineages in the serving leg (0: skip)")
+    ap.add_argument("--serve-steps", type=int, default=3, help="design steps per lineage in the serving leg")
+    ap.add_argument("--serve-rate", type=float, default=4.0, help="lineage arrivals per second (Poisson)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -360,11 +401,14 @@ def main():
             "refinements_mean": float(np.mean(res["batched"]["sweeps"])),
             "ch_rel_err_vs_fp64": res["batched"]["ch_rel_err_vs_fp64"],
             "over_plain_fp64": bt["value"] / f64["value"],
-            "fp64": dict(f64, roofline=roofline(res["fp64"]["prof"], hbm, kind), clocks=res["fp64"]["clocks"]),
+            "fp64": dict(f64, roofline=roofline(res["fp64"]["prof"], hbm, kind, "fp64"), clocks=res["fp64"]["clocks"],
+                         tiles=res["fp64"]["tiles"]),
             "mixed_single": dict(mx, ch_rel_err_vs_fp64=res["mixed"]["ch_rel_err_vs_fp64"]),
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": res["h2d"], "d2h_bytes_per_step": res["d2h"]},
-            "roofline": roofline(res["mixed"]["prof"], hbm, kind),
+            "roofline": roofline(res["mixed"]["prof"], hbm, kind, "mixed"), "tiles": res["mixed"]["tiles"],
             "gpu_launches": int(sum(res["batched"]["launches"])), "clocks": res["batched"]["clocks"]}
+    if "serving" in res:
+        line["serving"] = res["serving"]
     if world == 1 and not args.no_cpu:
         cb = cpu_sample(its_full=int(round(f64["iterations_max_mean"])))
         line["cpu_baseline"] = {"value": cb["value"], "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
