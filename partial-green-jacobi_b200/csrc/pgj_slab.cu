@@ -17,6 +17,7 @@
 // working on 32 lines at the same index touches distinct banks), the half spectrum as n rows of
 // nsp (even) complex values.
 #include "pgj_fft_engine.cuh"
+#include <cstdlib>
 #include <cstring>
 
 namespace pgj {
@@ -53,8 +54,10 @@ template <typename T>
 __device__ __forceinline__ T* real_view(cplx<T>* b) { return reinterpret_cast<T*>(b); }
 
 // ------------------------------------------------------------------------------------------ fxy
-template <typename T, typename U, int MODE>
-__global__ void __launch_bounds__(512, 2) k_fxy(const SlabArgs A) {
+// W4: blocks of at most 288 threads, four resident per SM (56 registers); otherwise up to 512
+// threads, two per SM.
+template <typename T, typename U, int MODE, bool W4>
+__global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int c = blockIdx.x, z = blockIdx.y, load = blockIdx.z;
@@ -189,8 +192,8 @@ __global__ void __launch_bounds__(512, 2) k_fxy(const SlabArgs A) {
 }
 
 // ----------------------------------------------------------------------------------------- ifxy
-template <typename T>
-__global__ void __launch_bounds__(512, 2) k_ifxy(const SlabArgs A) {
+template <typename T, bool W4>
+__global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int c = blockIdx.x, z = blockIdx.y, load = blockIdx.z;
@@ -299,17 +302,28 @@ bool slab_fits(const pgj_ctx* c) {
   return slab_smem(c->n, nsp, tsz) <= 110 * 1024;  // two blocks per SM
 }
 
+template <bool W4>
+static void set_slab_smem(int lim) {
+  cudaFuncSetAttribute(k_fxy<double, double, kSlabUpdate, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<double, double, kSlabInit, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<double, double, kSlabSync, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<float, float, kSlabUpdate, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<float, float, kSlabInit, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<float, float, kSlabSync, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_ifxy<double, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_ifxy<float, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+}
+
 int prepare_slab_kernels() {
-  const int lim = 112 * 1024;
-  cudaFuncSetAttribute(k_fxy<double, double, kSlabUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<double, double, kSlabInit>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<double, double, kSlabSync>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<float, float, kSlabUpdate>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<float, float, kSlabInit>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<float, float, kSlabSync>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_ifxy<double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_ifxy<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  set_slab_smem<false>(112 * 1024);
+  set_slab_smem<true>(112 * 1024);
   return check_launch();
+}
+
+// FP32 slabs of at most 288 threads take the four-per-SM register budget (PGJ_SLAB_W4=0: off)
+static bool slab_w4(int prec, int thr) {
+  const char* e = std::getenv("PGJ_SLAB_W4");
+  return prec == PGJ_FP32 && thr <= 288 && !(e && e[0] == '0');
 }
 
 static SlabArgs slab_args(pgj_ctx* c, int loads, int prec) {
@@ -337,17 +351,27 @@ int launch_fxy(pgj_ctx* c, int loads, int prec, int mode, void* u, cudaStream_t 
   const dim3 grid(3, c->n, loads);
   const int thr = slab_threads(c);
   const size_t smem = slab_smem(A.n, A.nsp, tsz);
+  const bool w4 = slab_w4(prec, thr);
   if (prec == PGJ_FP32) {
     switch (mode) {
-      case kSlabUpdate: k_fxy<float, float, kSlabUpdate><<<grid, thr, smem, s>>>(A); break;
-      case kSlabInit: k_fxy<float, float, kSlabInit><<<grid, thr, smem, s>>>(A); break;
-      default: k_fxy<float, float, kSlabSync><<<grid, thr, smem, s>>>(A); break;
+      case kSlabUpdate:
+        if (w4) k_fxy<float, float, kSlabUpdate, true><<<grid, thr, smem, s>>>(A);
+        else k_fxy<float, float, kSlabUpdate, false><<<grid, thr, smem, s>>>(A);
+        break;
+      case kSlabInit:
+        if (w4) k_fxy<float, float, kSlabInit, true><<<grid, thr, smem, s>>>(A);
+        else k_fxy<float, float, kSlabInit, false><<<grid, thr, smem, s>>>(A);
+        break;
+      default:
+        if (w4) k_fxy<float, float, kSlabSync, true><<<grid, thr, smem, s>>>(A);
+        else k_fxy<float, float, kSlabSync, false><<<grid, thr, smem, s>>>(A);
+        break;
     }
   } else {
     switch (mode) {
-      case kSlabUpdate: k_fxy<double, double, kSlabUpdate><<<grid, thr, smem, s>>>(A); break;
-      case kSlabInit: k_fxy<double, double, kSlabInit><<<grid, thr, smem, s>>>(A); break;
-      default: k_fxy<double, double, kSlabSync><<<grid, thr, smem, s>>>(A); break;
+      case kSlabUpdate: k_fxy<double, double, kSlabUpdate, false><<<grid, thr, smem, s>>>(A); break;
+      case kSlabInit: k_fxy<double, double, kSlabInit, false><<<grid, thr, smem, s>>>(A); break;
+      default: k_fxy<double, double, kSlabSync, false><<<grid, thr, smem, s>>>(A); break;
     }
   }
   return check_launch();
@@ -363,8 +387,12 @@ int launch_ifxy(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, cuda
   const dim3 grid(3, c->n, loads);
   const int thr = slab_threads(c);
   const size_t smem = slab_smem(A.n, A.nsp, tsz);
-  if (prec == PGJ_FP32) k_ifxy<float><<<grid, thr, smem, s>>>(A);
-  else k_ifxy<double><<<grid, thr, smem, s>>>(A);
+  if (prec == PGJ_FP32) {
+    if (slab_w4(prec, thr)) k_ifxy<float, true><<<grid, thr, smem, s>>>(A);
+    else k_ifxy<float, false><<<grid, thr, smem, s>>>(A);
+  } else {
+    k_ifxy<double, false><<<grid, thr, smem, s>>>(A);
+  }
   return check_launch();
 }
 
