@@ -318,6 +318,150 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
   }
 }
 
+// ---------------------------------------------------------------------------- FZ, n = 64
+// z pass of the fused recurrence at n = 64 with the line transforms in registers: a 64-point line
+// is an 8 x 8 four-step transform. Lane a of the 8 lanes of a line holds points z = a + 8b; it does
+// the 8-point DFT over b, multiplies by w64^(a k2), and a transpose through this warp's shared
+// memory hands lane t the values with k2 = t for the 8-point DFT over a; lane t then owns
+// kz = t + 8 k1. The inverse runs the same steps backwards. A warp owns four kx columns at one ky
+// (all three components); warps never wait on each other, so the only block barrier is the final
+// reduction. Same results as k_fz in fused mode (rz, beta and mean(s.w) by Parseval).
+constexpr int kFz64Line = 76;                 // complex slots per line (8 rows of 9, padded)
+constexpr int kFz64Comp = 4 * kFz64Line;      // one component of the warp's four lines
+
+template <typename T, int WPB, int MINB>
+__global__ void __launch_bounds__(WPB * 32, MINB) k_fz64(const GreenArgs A) {
+  using C = cplx<T>;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr int N = 64;
+  const int load = blockIdx.y;
+  if (!load_on(A, load)) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int l = lane >> 3, t = lane & 7;
+  const int ns = A.ns, nsp = A.nsp;
+  const int groups = (ns + 3) >> 2;
+  const int w = blockIdx.x * WPB + warp;
+  const int ky = w / groups, kx = (w - ky * groups) * 4 + l;
+  const bool valid = ky < N && kx < ns;
+  C* buf = reinterpret_cast<C*>(smem_raw) + (warp * 3 * 4 + l) * kFz64Line;  // + c * kFz64Comp
+  double* red = reinterpret_cast<double*>(reinterpret_cast<C*>(smem_raw) + WPB * 3 * kFz64Comp);
+  const size_t plane = size_t(N) * N * nsp;
+  C* sp = reinterpret_cast<C*>(A.spec) + size_t(load) * 3 * plane;
+  const C* tw = reinterpret_cast<const C*>(A.tw);
+  const C zero = cmk<C>(0.0, 0.0);
+  const size_t col = size_t(ky) * nsp + kx;  // offset of (z = 0, ky, kx) in one component
+  // forward: DFT over b, twiddle, column write (row k2, column t)
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    C v[8];
+#pragma unroll
+    for (int b = 0; b < 8; ++b) v[b] = valid ? sp[c * plane + size_t(t + 8 * b) * N * nsp + col] : zero;
+    Radix<T, 8>::run(v, false);
+#pragma unroll
+    for (int k2 = 1; k2 < 8; ++k2) v[k2] = cmul(v[k2], __ldg(&tw[t * k2]));
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) buf[c * kFz64Comp + k2 * 9 + t] = v[k2];
+  }
+  __syncwarp();
+  // DFT over a of row t; X[kz = t + 8 k1] goes to (row k1, column t)
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    C v[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = buf[c * kFz64Comp + t * 9 + j];
+    Radix<T, 8>::run(v, false);
+    __syncwarp();  // every lane has read its row before the column writes
+#pragma unroll
+    for (int k1 = 0; k1 < 8; ++k1) buf[c * kFz64Comp + k1 * 9 + t] = v[k1];
+  }
+  // symbol multiply and the Parseval sums on the lane's own column
+  const T* sym = reinterpret_cast<const T*>(A.sym);
+  const C* sh = reinterpret_cast<const C*>(A.shat);
+  const size_t Nh = size_t(N) * N * ns;
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  if (valid) {
+    const double wgt = (kx == 0 || kx == N / 2) ? 1.0 : 2.0;
+    const T m0 = T(A.scal[load].mean_r[0]), m1 = T(A.scal[load].mean_r[1]), m2 = T(A.scal[load].mean_r[2]);
+#pragma unroll 2
+    for (int k1 = 0; k1 < 8; ++k1) {
+      const int kz = t + 8 * k1;
+      const size_t kk = (size_t(kz) * N + ky) * ns + kx;
+      const T c0 = sym[kk], c1 = sym[Nh + kk], c2 = sym[2 * Nh + kk];
+      const T c3 = sym[3 * Nh + kk], c4 = sym[4 * Nh + kk], c5 = sym[5 * Nh + kk];
+      const size_t ks = size_t(kz) * N * nsp + col;
+      const C s0 = sh[ks], s1 = sh[plane + ks], s2 = sh[2 * plane + ks];
+      C* px = buf + k1 * 9 + t;
+      C x = px[0], y = px[kFz64Comp], zv = px[2 * kFz64Comp];
+      x.x -= m0 * s0.x; x.y -= m0 * s0.y;
+      y.x -= m1 * s1.x; y.y -= m1 * s1.y;
+      zv.x -= m2 * s2.x; zv.y -= m2 * s2.y;
+      C wx, wy, wz;
+      wx.x = c0 * x.x + c3 * y.x + c4 * zv.x; wx.y = c0 * x.y + c3 * y.y + c4 * zv.y;
+      wy.x = c3 * x.x + c1 * y.x + c5 * zv.x; wy.y = c3 * x.y + c1 * y.y + c5 * zv.y;
+      wz.x = c4 * x.x + c5 * y.x + c2 * zv.x; wz.y = c4 * x.y + c5 * y.y + c2 * zv.y;
+      acc[0] += wgt * (double(x.x) * wx.x + double(x.y) * wx.y + double(y.x) * wy.x + double(y.y) * wy.y +
+                       double(zv.x) * wz.x + double(zv.y) * wz.y);
+      acc[1] += wgt * (double(wx.x) * s0.x + double(wx.y) * s0.y);
+      acc[2] += wgt * (double(wy.x) * s1.x + double(wy.y) * s1.y);
+      acc[3] += wgt * (double(wz.x) * s2.x + double(wz.y) * s2.y);
+      px[0] = wx; px[kFz64Comp] = wy; px[2 * kFz64Comp] = wz;
+    }
+  }
+  // inverse: DFT over k1 of the own column, twiddle, column write (row a, column t); then the
+  // DFT over k2 of row t gives z = t + 8 b
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    C v[8];
+#pragma unroll
+    for (int k1 = 0; k1 < 8; ++k1) v[k1] = buf[c * kFz64Comp + k1 * 9 + t];
+    Radix<T, 8>::run(v, true);
+#pragma unroll
+    for (int a = 1; a < 8; ++a) {
+      C wt = __ldg(&tw[t * a]);
+      wt.y = -wt.y;
+      v[a] = cmul(v[a], wt);
+    }
+#pragma unroll
+    for (int a = 0; a < 8; ++a) buf[c * kFz64Comp + a * 9 + t] = v[a];
+  }
+  __syncwarp();
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    C v[8];
+#pragma unroll
+    for (int k2 = 0; k2 < 8; ++k2) v[k2] = buf[c * kFz64Comp + t * 9 + k2];
+    Radix<T, 8>::run(v, true);
+    if (valid) {
+#pragma unroll
+      for (int b = 0; b < 8; ++b) sp[c * plane + size_t(t + 8 * b) * N * nsp + col] = v[b];
+    }
+  }
+  // Parseval partials -> last block: rz, beta, mean(s.w) (as k_fz)
+  const int tid = threadIdx.x;
+  block_sum<4>(acc, red);
+  const int nblk = gridDim.x, blk = blockIdx.x;
+  double* part = A.partials + size_t(load) * kPartialQ * kMaxPartials;
+  if (tid == 0)
+    for (int k = 0; k < 4; ++k) part[k * kMaxPartials + blk] = acc[k];
+  LoadScalars& S = A.scal[load];
+  if (!last_block(&S.ticket[kTicketFZ], nblk)) return;
+  if (tid < 32) {
+    const double rzn = warp_sum_partials(part, nblk);
+    double mz[3];
+    for (int k = 0; k < 3; ++k) mz[k] = warp_sum_partials(part + (k + 1) * kMaxPartials, nblk);
+    if (tid == 0) {
+      if (A.init) {
+        S.beta = 0.0;
+      } else {
+        const double rz = S.rz;
+        S.beta = rzn / (rz != 0.0 ? rz : 1.0);
+      }
+      S.rz = rzn;
+      for (int k = 0; k < 3; ++k) S.mean_z[k] = mz[k] / double(size_t(N) * N * N);
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------- IFX
 // block (3 rb/2 lines, by): C2R of rb rows, two rows per complex line; s.w and its sums.
 template <typename T>
@@ -408,6 +552,21 @@ static size_t smem_x(const pgj_ctx* c, size_t cb) {
 static size_t smem_y(const pgj_ctx* c, size_t cb) { return 2 * size_t(c->fg.kcy) * (c->n + 1) * cb; }
 static size_t smem_z(const pgj_ctx* c, size_t cb) { return 2 * 3 * size_t(c->fg.kcz) * (c->n + 1) * cb + 32 * 4 * 8 + 64; }
 
+template <typename T> constexpr int fz64_warps() { return sizeof(T) == 4 ? 8 : 4; }  // warps per block
+template <typename T>
+static size_t fz64_smem() { return size_t(fz64_warps<T>()) * 3 * kFz64Comp * 2 * sizeof(T) + 32 * 4 * 8 + 64; }
+
+template <typename T>
+static int run_fz64(pgj_ctx* c, int loads, const GreenArgs& A, cudaStream_t s) {
+  constexpr int WPB = fz64_warps<T>();
+  const int warps = ((c->ns + 3) / 4) * c->n;  // per load
+  const dim3 grid((warps + WPB - 1) / WPB, loads);
+  const char* e = std::getenv("PGJ_FZ64_MINB");  // default: three blocks per SM (register cap); 1: unbounded
+  if (e && e[0] == '1') k_fz64<T, WPB, 1><<<grid, WPB * 32, fz64_smem<T>(), s>>>(A);
+  else k_fz64<T, WPB, 3><<<grid, WPB * 32, fz64_smem<T>(), s>>>(A);
+  return check_launch();
+}
+
 template <typename T>
 static int set_smem_limits() {
   const int lim = 220 * 1024;  // below the 227 KB opt-in less the static shared memory
@@ -416,6 +575,8 @@ static int set_smem_limits() {
   cudaFuncSetAttribute(k_fy<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fz<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_ifx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fz64<T, fz64_warps<T>(), 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fz64<T, fz64_warps<T>(), 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   return check_launch();
 }
 
@@ -485,6 +646,9 @@ int launch_fz_fused(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s) 
   A.finalize_fz = 1;
   A.fused = 1;
   A.shat = c->shat;
+  const char* e = std::getenv("PGJ_FZ64");
+  if (c->n == 64 && !(e && e[0] == '0'))  // line transforms in registers (PGJ_FZ64=0: generic pass)
+    return prec == PGJ_FP32 ? run_fz64<float>(c, loads, A, s) : run_fz64<double>(c, loads, A, s);
   return prec == PGJ_FP32 ? run_green_pass<float>(c, loads, A, s, 2) : run_green_pass<double>(c, loads, A, s, 2);
 }
 

@@ -343,6 +343,28 @@ def test_fused_iteration_matches_unfused(pkg, n, prec, emin):
     assert rel(C1, C0) < (1e-10 if prec == "fp64" else 1e-7), rel(C1, C0)
 
 
+@pytest.mark.parametrize("prec", ["fp64", "mixed"])
+def test_register_z_pass_matches_generic_z_pass(pkg, prec, monkeypatch):
+    """n = 64: the z pass with the line transforms in registers against the generic shared-memory
+    pass (both in the four-kernel iteration)."""
+    n = 64
+    lam, mu = pkg.PAPER_MEDIUM
+    a = dev(pkg.baseline_design(n, seed=5, emin=1e-4))
+    out = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("PGJ_FZ64", flag)
+        op = pkg.Operator(n, 6, lam, mu, precision=prec)
+        op.set_material(a)
+        op.set_alpha(0.5)
+        u = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")
+        infos, st = op.solve(np.eye(6), 1e-8, u)
+        assert st == 0, (flag, infos)
+        out[flag] = (op.effective_tensor(u).cpu().numpy(), np.array([i["iterations"] for i in infos]))
+    (C0, i0), (C1, i1) = out["0"], out["1"]
+    assert np.all(np.abs(i1 - i0) <= np.maximum(1, np.ceil(0.02 * i0))), (i0, i1)
+    assert rel(C1, C0) < (1e-10 if prec == "fp64" else 1e-7), rel(C1, C0)
+
+
 def test_fused_iteration_falls_back_when_the_slab_does_not_fit(pkg):
     op = pkg.Operator(128, 1, *pkg.PAPER_MEDIUM)
     assert not op.fused_iteration
