@@ -55,7 +55,8 @@ static Layout make_layout(int n, int L, int prec) {
   y.macros = take(sizeof(double) * 6 * size_t(L));
   y.cond = take(64);
   y.aux = take(sizeof(double) * kAuxDoubles);
-  y.tw = take(size_t(n) * (sizeof(double2) + sizeof(float2)));
+  // twiddles (double2[n], float2[n]) and the per-axis Green factors (float4[n]: m, v, d)
+  y.tw = take(size_t(n) * (sizeof(double2) + sizeof(float2) + sizeof(float4)));
   const size_t pslots = size_t(4 * L > 24 ? 4 * L : 24);
   y.partials = take(sizeof(double) * pslots * kMaxPartials);
   y.a = take(sizeof(double) * N);
