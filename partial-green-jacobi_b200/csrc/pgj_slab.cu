@@ -53,10 +53,39 @@ constexpr int kMaxBodyRunsSlab = 4100;  // same bound as the unfused loop body
 template <typename T>
 __device__ __forceinline__ T* real_view(cplx<T>* b) { return reinterpret_cast<T*>(b); }
 
+// n = 64: a 64-point line as an 8 x 8 four-step transform held by 8 lanes (lane t holds points
+// t + 8b), with the transpose through the line's own shared-memory region L (rows of 9, 76 slots).
+// Forward from registers v[b] = x[t + 8b]: on return v[k1] = X[t + 8 k1]. Inverse from
+// v[k1] = X[t + 8 k1]: on return v[b] = x[t + 8 b] (unnormalised). The caller's eight lanes of the
+// line must be converged; L must not be read by other lanes meanwhile.
+constexpr int kLine64 = 76;
+template <typename T>
+__device__ __forceinline__ void line64(cplx<T> (&v)[8], cplx<T>* L, int t, const cplx<T>* __restrict__ tw, bool inv) {
+  using C = cplx<T>;
+  Radix<T, 8>::run(v, inv);
+#pragma unroll
+  for (int k = 1; k < 8; ++k) {
+    C w = __ldg(&tw[t * k]);
+    if (inv) w.y = -w.y;
+    v[k] = cmul(v[k], w);
+  }
+  __syncwarp();
+#pragma unroll
+  for (int k = 0; k < 8; ++k) L[k * 9 + t] = v[k];
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < 8; ++j) v[j] = L[t * 9 + j];
+  Radix<T, 8>::run(v, inv);
+  __syncwarp();
+}
+
 // ------------------------------------------------------------------------------------------ fxy
 // W4: blocks of at most 288 threads, four resident per SM (56 registers); otherwise up to 512
 // threads, two per SM.
-template <typename T, typename U, int MODE, bool W4>
+// R64 (n = 64, 288 threads): x and y lines as register four-step transforms (line64); shared
+// memory holds 36 lines of 76 complex values (packed x lines, then per-warp transpose space) and
+// the n x nsp half-spectrum rows.
+template <typename T, typename U, int MODE, bool W4, bool R64>
 __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -67,7 +96,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int nn = n * n;
   C* b0 = reinterpret_cast<C*>(smem_raw);
-  C* b1 = b0 + size_t(n) * nsp;
+  C* b1 = b0 + (R64 ? 36 * kLine64 : size_t(n) * nsp);
   double* red = reinterpret_cast<double*>(b1 + size_t(n) * nsp);
   const size_t N = size_t(nn) * n, N3 = 3 * N;
   const size_t node0 = size_t(z) * nn;
@@ -75,7 +104,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   T* r = reinterpret_cast<T*>(A.r) + off;
   const double* sc = A.scale + 3 * node0 + c;
   T* packed = real_view<T>(b0);
-  const int lpx = n + 1;  // pitch of the packed x lines
+  const int lpx = R64 ? kLine64 : n + 1;  // pitch of the packed x lines
   double acc[2] = {0.0, 0.0};
   const double alpha = MODE == kSlabUpdate ? S.alpha : 0.0;
   const T a = T(alpha);
@@ -125,8 +154,26 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   }
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_lines<T, true>(b0, b1, n / 2, lpx, 1, A.plan, A.div_nh, tw, false, tid, nthr);
-  C* oth = res == b0 ? b1 : b0;
+  C* res;
+  C* oth;
+  const int warp = tid >> 5, li = (tid & 31) >> 3, t8 = tid & 7;
+  if constexpr (R64) {
+    if (warp < 8) {  // 32 packed x lines, four per warp, eight lanes per line
+      C* L = b0 + (4 * warp + li) * kLine64;
+      C v[8];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) v[b] = L[t8 + 8 * b];
+      line64<T>(v, L, t8, tw, false);
+#pragma unroll
+      for (int k1 = 0; k1 < 8; ++k1) L[t8 + 8 * k1] = v[k1];
+    }
+    __syncthreads();
+    res = b0;
+    oth = b1;
+  } else {
+    res = fft_lines<T, true>(b0, b1, n / 2, lpx, 1, A.plan, A.div_nh, tw, false, tid, nthr);
+    oth = res == b0 ? b1 : b0;
+  }
   // split the packed transforms: row rho = 2l (real part) and 2l+1 (imaginary part)
   for (int i = tid; i < n * ns; i += nthr) {
     const int rho = fdiv(i, A.div_ns), k = i - rho * ns;
@@ -140,11 +187,27 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   }
   __syncthreads();
   // y transform of the ns columns
-  C* res2 = fft_lines<T, true>(oth, res, ns, 1, nsp, A.plan, A.div_ns, tw, false, tid, nthr);
   C* sp = reinterpret_cast<C*>(A.spec) + ((size_t(load) * 3 + c) * n + z) * size_t(n) * nsp;
-  for (int i = tid; i < n * ns; i += nthr) {
-    const int ky = fdiv(i, A.div_ns), kx = i - ky * ns;
-    sp[size_t(ky) * nsp + kx] = res2[ky * nsp + kx];
+  if constexpr (R64) {
+    // columns four per warp (nine warps), straight from the rows to the spectrum in global memory
+    const int col = 4 * warp + li;
+    const bool valid = col < ns;
+    C* L = b0 + (4 * warp + li) * kLine64;  // free once the split has read the packed lines
+    C v[8];
+    const C zero = cmk<C>(0.0, 0.0);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) v[b] = valid ? oth[(t8 + 8 * b) * nsp + col] : zero;
+    line64<T>(v, L, t8, tw, false);
+    if (valid) {
+#pragma unroll
+      for (int k1 = 0; k1 < 8; ++k1) sp[size_t(t8 + 8 * k1) * nsp + col] = v[k1];
+    }
+  } else {
+    C* res2 = fft_lines<T, true>(oth, res, ns, 1, nsp, A.plan, A.div_ns, tw, false, tid, nthr);
+    for (int i = tid; i < n * ns; i += nthr) {
+      const int ky = fdiv(i, A.div_ns), kx = i - ky * ns;
+      sp[size_t(ky) * nsp + kx] = res2[ky * nsp + kx];
+    }
   }
   if (MODE == kSlabInit) return;
 
@@ -192,7 +255,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
 }
 
 // ----------------------------------------------------------------------------------------- ifxy
-template <typename T, bool W4>
+template <typename T, bool W4, bool R64>
 __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -210,21 +273,43 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
   if (!S.active) return;
   const int n = A.n, ns = A.ns, nsp = A.nsp;
   const int nn = n * n;
-  const int lpx = n + 1;  // pitch of the packed x lines
+  const int lpx = R64 ? kLine64 : n + 1;  // pitch of the packed x lines
   C* b0 = reinterpret_cast<C*>(smem_raw);
-  C* b1 = b0 + size_t(n) * nsp;
+  C* b1 = b0 + (R64 ? 36 * kLine64 : size_t(n) * nsp);
   const C* sp = reinterpret_cast<const C*>(A.spec) + ((size_t(load) * 3 + c) * n + z) * size_t(n) * nsp;
-  batched_copy<8>(tid, nthr, n * ns, [&](int i) {
-    const int ky = fdiv(i, A.div_ns), kx = i - ky * ns;
-    return sp[size_t(ky) * nsp + kx];
-  }, [&](int i, C v) {
-    const int ky = fdiv(i, A.div_ns), kx = i - ky * ns;
-    b0[ky * nsp + kx] = v;
-  });
-  __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
-  C* res = fft_lines<T, true>(b0, b1, ns, 1, nsp, A.plan, A.div_ns, tw, true, tid, nthr);
-  C* oth = res == b0 ? b1 : b0;
+  const int warp = tid >> 5, li = (tid & 31) >> 3, t8 = tid & 7;
+  C* res;
+  C* oth;
+  if constexpr (R64) {
+    // inverse y of four columns per warp straight from global memory into the rows (b1)
+    const int col = 4 * warp + li;
+    const bool valid = col < ns;
+    C* L = b0 + (4 * warp + li) * kLine64;
+    C v[8];
+    const C zero = cmk<C>(0.0, 0.0);
+#pragma unroll
+    for (int k1 = 0; k1 < 8; ++k1) v[k1] = valid ? sp[size_t(t8 + 8 * k1) * nsp + col] : zero;
+    line64<T>(v, L, t8, tw, true);
+    if (valid) {
+#pragma unroll
+      for (int b = 0; b < 8; ++b) b1[(t8 + 8 * b) * nsp + col] = v[b];
+    }
+    __syncthreads();
+    res = b1;
+    oth = b0;
+  } else {
+    batched_copy<8>(tid, nthr, n * ns, [&](int i) {
+      const int ky = fdiv(i, A.div_ns), kx = i - ky * ns;
+      return sp[size_t(ky) * nsp + kx];
+    }, [&](int i, C v) {
+      const int ky = fdiv(i, A.div_ns), kx = i - ky * ns;
+      b0[ky * nsp + kx] = v;
+    });
+    __syncthreads();
+    res = fft_lines<T, true>(b0, b1, ns, 1, nsp, A.plan, A.div_ns, tw, true, tid, nthr);
+    oth = res == b0 ? b1 : b0;
+  }
   // C2R packing: line l = A + i B over the full x range (rows 2l, 2l+1 Hermitian-extended,
   // imaginary parts of the DC and Nyquist bins dropped)
   for (int i = tid; i < (n / 2) * n; i += nthr) {
@@ -248,7 +333,22 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
     oth[l * lpx + k] = zz;
   }
   __syncthreads();
-  C* res2 = fft_lines<T, true>(oth, res, n / 2, lpx, 1, A.plan, A.div_nh, tw, true, tid, nthr);
+  C* res2;
+  if constexpr (R64) {
+    if (warp < 8) {
+      C* L = oth + (4 * warp + li) * kLine64;
+      C v[8];
+#pragma unroll
+      for (int k1 = 0; k1 < 8; ++k1) v[k1] = L[t8 + 8 * k1];
+      line64<T>(v, L, t8, tw, true);
+#pragma unroll
+      for (int b = 0; b < 8; ++b) L[t8 + 8 * b] = v[b];
+    }
+    __syncthreads();
+    res2 = oth;
+  } else {
+    res2 = fft_lines<T, true>(oth, res, n / 2, lpx, 1, A.plan, A.div_nh, tw, true, tid, nthr);
+  }
   const T* wv = real_view<T>(res2);
   const size_t node0 = size_t(z) * nn;
   const size_t off = size_t(load) * 3 * size_t(nn) * n + 3 * node0 + c;
@@ -284,6 +384,8 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
 
 // ------------------------------------------------------------------------------------ host side
 static size_t slab_smem(int n, int nsp, size_t tsz) { return 2 * size_t(n) * nsp * 2 * tsz + 32 * 2 * 8 + 64; }
+// R64: 36 lines of kLine64 complex values, then the n x nsp rows, then the reduction
+static size_t slab_smem64(int nsp, size_t tsz) { return (36 * size_t(kLine64) + 64 * size_t(nsp)) * 2 * tsz + 32 * 2 * 8 + 64; }
 
 static int slab_threads(const pgj_ctx* c) {
   int minr = 8;
@@ -302,21 +404,21 @@ bool slab_fits(const pgj_ctx* c) {
   return slab_smem(c->n, nsp, tsz) <= 110 * 1024;  // two blocks per SM
 }
 
-template <bool W4>
-static void set_slab_smem(int lim) {
-  cudaFuncSetAttribute(k_fxy<double, double, kSlabUpdate, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<double, double, kSlabInit, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<double, double, kSlabSync, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<float, float, kSlabUpdate, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<float, float, kSlabInit, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<float, float, kSlabSync, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_ifxy<double, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_ifxy<float, W4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+template <typename T, typename U, bool W4, bool R64>
+static void set_fxy_smem(int lim) {
+  cudaFuncSetAttribute(k_fxy<T, U, kSlabUpdate, W4, R64>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<T, U, kSlabInit, W4, R64>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<T, U, kSlabSync, W4, R64>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_ifxy<T, W4, R64>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 
 int prepare_slab_kernels() {
-  set_slab_smem<false>(112 * 1024);
-  set_slab_smem<true>(112 * 1024);
+  const int lim = 112 * 1024;
+  set_fxy_smem<double, double, false, false>(lim);
+  set_fxy_smem<double, double, false, true>(lim);
+  set_fxy_smem<float, float, false, false>(lim);
+  set_fxy_smem<float, float, true, false>(lim);
+  set_fxy_smem<float, float, true, true>(lim);
   return check_launch();
 }
 
@@ -324,6 +426,13 @@ int prepare_slab_kernels() {
 static bool slab_w4(int prec, int thr) {
   const char* e = std::getenv("PGJ_SLAB_W4");
   return prec == PGJ_FP32 && thr <= 288 && !(e && e[0] == '0');
+}
+
+// n = 64 with 288 threads: register line transforms (PGJ_SLAB64=0: the generic passes)
+static bool slab_r64(const pgj_ctx* c, int prec, int thr) {
+  const char* e = std::getenv("PGJ_SLAB64");
+  (void)prec;
+  return c->n == 64 && thr == 288 && !(e && e[0] == '0');
 }
 
 static SlabArgs slab_args(pgj_ctx* c, int loads, int prec) {
@@ -344,35 +453,30 @@ static SlabArgs slab_args(pgj_ctx* c, int loads, int prec) {
 }
 
 // mode: kSlabUpdate (u in `u`: FP64 x, or the FP32 correction d), kSlabInit, kSlabSync
+template <typename T, typename U, bool W4, bool R64>
+static void fxy_kernel(int mode, dim3 grid, int thr, size_t smem, cudaStream_t s, const SlabArgs& A) {
+  switch (mode) {
+    case kSlabUpdate: k_fxy<T, U, kSlabUpdate, W4, R64><<<grid, thr, smem, s>>>(A); break;
+    case kSlabInit: k_fxy<T, U, kSlabInit, W4, R64><<<grid, thr, smem, s>>>(A); break;
+    default: k_fxy<T, U, kSlabSync, W4, R64><<<grid, thr, smem, s>>>(A); break;
+  }
+}
+
 int launch_fxy(pgj_ctx* c, int loads, int prec, int mode, void* u, cudaStream_t s) {
   SlabArgs A = slab_args(c, loads, prec);
   A.u = u;
   const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
   const dim3 grid(3, c->n, loads);
   const int thr = slab_threads(c);
-  const size_t smem = slab_smem(A.n, A.nsp, tsz);
-  const bool w4 = slab_w4(prec, thr);
+  const bool r64 = slab_r64(c, prec, thr);
+  const size_t smem = r64 ? slab_smem64(A.nsp, tsz) : slab_smem(A.n, A.nsp, tsz);
   if (prec == PGJ_FP32) {
-    switch (mode) {
-      case kSlabUpdate:
-        if (w4) k_fxy<float, float, kSlabUpdate, true><<<grid, thr, smem, s>>>(A);
-        else k_fxy<float, float, kSlabUpdate, false><<<grid, thr, smem, s>>>(A);
-        break;
-      case kSlabInit:
-        if (w4) k_fxy<float, float, kSlabInit, true><<<grid, thr, smem, s>>>(A);
-        else k_fxy<float, float, kSlabInit, false><<<grid, thr, smem, s>>>(A);
-        break;
-      default:
-        if (w4) k_fxy<float, float, kSlabSync, true><<<grid, thr, smem, s>>>(A);
-        else k_fxy<float, float, kSlabSync, false><<<grid, thr, smem, s>>>(A);
-        break;
-    }
+    if (r64) fxy_kernel<float, float, true, true>(mode, grid, thr, smem, s, A);
+    else if (slab_w4(prec, thr)) fxy_kernel<float, float, true, false>(mode, grid, thr, smem, s, A);
+    else fxy_kernel<float, float, false, false>(mode, grid, thr, smem, s, A);
   } else {
-    switch (mode) {
-      case kSlabUpdate: k_fxy<double, double, kSlabUpdate, false><<<grid, thr, smem, s>>>(A); break;
-      case kSlabInit: k_fxy<double, double, kSlabInit, false><<<grid, thr, smem, s>>>(A); break;
-      default: k_fxy<double, double, kSlabSync, false><<<grid, thr, smem, s>>>(A); break;
-    }
+    if (r64) fxy_kernel<double, double, false, true>(mode, grid, thr, smem, s, A);
+    else fxy_kernel<double, double, false, false>(mode, grid, thr, smem, s, A);
   }
   return check_launch();
 }
@@ -386,12 +490,15 @@ int launch_ifxy(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, cuda
   const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
   const dim3 grid(3, c->n, loads);
   const int thr = slab_threads(c);
-  const size_t smem = slab_smem(A.n, A.nsp, tsz);
+  const bool r64 = slab_r64(c, prec, thr);
+  const size_t smem = r64 ? slab_smem64(A.nsp, tsz) : slab_smem(A.n, A.nsp, tsz);
   if (prec == PGJ_FP32) {
-    if (slab_w4(prec, thr)) k_ifxy<float, true><<<grid, thr, smem, s>>>(A);
-    else k_ifxy<float, false><<<grid, thr, smem, s>>>(A);
+    if (r64) k_ifxy<float, true, true><<<grid, thr, smem, s>>>(A);
+    else if (slab_w4(prec, thr)) k_ifxy<float, true, false><<<grid, thr, smem, s>>>(A);
+    else k_ifxy<float, false, false><<<grid, thr, smem, s>>>(A);
   } else {
-    k_ifxy<double, false><<<grid, thr, smem, s>>>(A);
+    if (r64) k_ifxy<double, false, true><<<grid, thr, smem, s>>>(A);
+    else k_ifxy<double, false, false><<<grid, thr, smem, s>>>(A);
   }
   return check_launch();
 }

@@ -345,14 +345,16 @@ def test_fused_iteration_matches_unfused(pkg, n, prec, emin):
 
 @pytest.mark.parametrize("prec", ["fp64", "mixed"])
 def test_register_z_pass_matches_generic_z_pass(pkg, prec, monkeypatch):
-    """n = 64: the z pass with the line transforms in registers against the generic shared-memory
-    pass (both in the four-kernel iteration)."""
+    """n = 64: the z pass and the slab transforms with the line transforms in registers against the
+    generic shared-memory passes (both in the four-kernel iteration)."""
     n = 64
     lam, mu = pkg.PAPER_MEDIUM
     a = dev(pkg.baseline_design(n, seed=5, emin=1e-4))
     out = {}
     for flag in ("0", "1"):
+        # "0": generic shared-memory passes; "1": register line transforms in the z pass and slabs
         monkeypatch.setenv("PGJ_FZ64", flag)
+        monkeypatch.setenv("PGJ_SLAB64", flag)
         op = pkg.Operator(n, 6, lam, mu, precision=prec)
         op.set_material(a)
         op.set_alpha(0.5)
