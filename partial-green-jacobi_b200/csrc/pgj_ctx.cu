@@ -74,6 +74,7 @@ static Layout make_layout(int n, int L, int prec) {
   y.sw = take(tsz * N3 * L);
   y.spec = take(2 * tsz * 3 * size_t(n) * n * nsp * L);
   y.shat = take(2 * tsz * 3 * size_t(n) * n * nsp);
+  y.scale32 = take(prec == PGJ_FP32 ? sizeof(float) * N3 : 0);
   y.total = o;
   return y;
 }
@@ -111,10 +112,15 @@ static int capture_iteration(pgj_ctx* c, int L, cudaStream_t s, cudaGraphConditi
 
 // First direction p = M r of a recurrence (the masks are set): unfused Green + p = z, or the fused
 // form, which first refreshes DFT(s) in case the scale field was rewritten through its view.
+static long long first_direction_launches(const pgj_ctx* c) {
+  return c->fused ? (c->prec == PGJ_FP32 ? 7 : 6) : 6;  // DFT(s) (3) [+ FP32 scale] + 3, or Green (5) + p
+}
+
 static int capture_first_direction(pgj_ctx* c, int L, cudaStream_t s) {
   int st;
   if (c->fused) {
     if ((st = build_shat(c, s))) return st;
+    if (c->prec == PGJ_FP32 && (st = launch_scale32(c, s))) return st;
     if ((st = launch_fxy(c, L, c->prec, kSlabInitL, nullptr, s))) return st;
     if ((st = launch_fz_fused(c, L, c->prec, true, s))) return st;
     return launch_ifxy(c, L, c->prec, true, s, 0, false);
@@ -414,6 +420,7 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
   c->r64 = precision == PGJ_FP32 ? reinterpret_cast<double*>(b + y.r64) : nullptr;
   c->r = b + y.r; c->p = b + y.p; c->q = b + y.q; c->sw = b + y.sw; c->spec = b + y.spec;
   c->shat = b + y.shat;
+  c->scale32 = precision == PGJ_FP32 ? reinterpret_cast<float*>(b + y.scale32) : nullptr;
   c->partials = reinterpret_cast<double*>(b + y.partials);
   c->scal_out = reinterpret_cast<LoadScalars*>(b + y.scal);
   c->scal_in = c->scal_out + loads;
@@ -592,12 +599,14 @@ int pgj_solve_wait(pgj_ctx* c, pgj_load_info* info, void* stream) {
   }
   const long long attempts = cnt[4] + 1;
   // loop body: operator, update, 5 Green passes, p update (fused: operator, fxy, fz, ifxy), plus the
-  // IF-condition kernel of the reliable-update form; the first direction is 7 kernels either way
+  // IF-condition kernel of the reliable-update form; the first direction is 6 kernels (fused FP32:
+  // 7, with the FP32 scale copy) after the mask / recurrence-start kernel
   const long long body = (c->fused ? 4 : 8) + (c->prec == PGJ_FP32 ? 1 : 0);
+  const long long first = first_direction_launches(c);
   if (c->prec == PGJ_FP32)  // rel start, first direction, fold, certify, decide; 3 per replacement
-    c->last_launches = 2 + 3 + attempts * (7 + 1 + 3 + 1) + body * cnt[5] + 3LL * cnt[3];
+    c->last_launches = 2 + 3 + attempts * (1 + first + 1 + 3 + 1) + body * cnt[5] + 3LL * cnt[3];
   else  // init mask, first direction, certify, decide
-    c->last_launches = 2 + 3 + attempts * (7 + 3 + 1) + body * cnt[5];
+    c->last_launches = 2 + 3 + attempts * (1 + first + 3 + 1) + body * cnt[5];
   c->last_refinements = c->prec == PGJ_FP32 ? 1 + cnt[3] : 1;
   if (cnt[2]) return PGJ_ERR_TIMEOUT;
   if (cnt[1]) return PGJ_ERR_ITERATION_CAP;
@@ -657,8 +666,8 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
       if ((e = cudaGraphLaunch(c->graphs->attempt, s)) != cudaSuccess) return set_cuda_error(e);
       ++sweeps;
       if ((e = read_state(true)) != cudaSuccess) return set_cuda_error(e);
-      // sweep: inner start + first direction (6), loop bodies, x += d, 3 certification kernels
-      launches += 1 + 6 + (c->fused ? 4LL : 8LL) * body[0] + 1 + 3;
+      // sweep: inner start + first direction, loop bodies, x += d, 3 certification kernels
+      launches += 1 + first_direction_launches(c) + (c->fused ? 4LL : 8LL) * body[0] + 1 + 3;
       if (body[1]) { capped_by_bound = true; break; }
     }
   } else {
@@ -666,9 +675,9 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
       if ((e = cudaGraphLaunch(c->graphs->attempt, s)) != cudaSuccess) return set_cuda_error(e);
       if ((e = read_state(true)) != cudaSuccess) return set_cuda_error(e);
       if (c->prec == PGJ_FP32)  // rel start + first direction, bodies, 3 per replacement, fold + certify
-        launches += 7 + (c->fused ? 5LL : 9LL) * body[0] + 3LL * body[3] + 1 + 3;
+        launches += 1 + first_direction_launches(c) + (c->fused ? 5LL : 9LL) * body[0] + 3LL * body[3] + 1 + 3;
       else  // attempt: init mask + first direction, loop bodies, 3 certification kernels
-        launches += 7 + (c->fused ? 4LL : 8LL) * body[0] + 3;
+        launches += 1 + first_direction_launches(c) + (c->fused ? 4LL : 8LL) * body[0] + 3;
       if (body[1]) { capped_by_bound = true; break; }
       bool all, anybad, capped;
       evaluate(all, anybad, capped);
@@ -788,7 +797,8 @@ int pgj_profile_iteration(pgj_ctx* c, int loads, const double* macros, int reps,
   const double sz = prec == PGJ_FP32 ? 4.0 : 8.0;     // bytes per real of the inner precision
   const double V = double(N3) * sz * loads;           // one DOF vector over all loads
   const double S = double(Nh) * 3 * 2 * sz * loads;  // one complex half spectrum over all loads
-  const double sc = double(N3) * 8.0;                 // scale field (FP64)
+  // scale field: FP64, or the FP32 planar copy the fused FP32 slab kernels read
+  const double sc = double(N3) * ((fused && prec == PGJ_FP32) ? 4.0 : 8.0);
   const double ub = prec == PGJ_FP32 ? V : 2 * V;   // iterate: FP64 x or the inner-precision correction
   const double fused_algo[PGJ_PROFILE_KERNELS] = {
       2 * V + 8.0 * N,                            // operator: read p (+a), write q

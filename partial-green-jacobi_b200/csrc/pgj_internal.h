@@ -70,7 +70,7 @@ constexpr int kAuxPartials = 128;
 constexpr int kAuxDoubles = kAuxPartials + kMaxPartials;
 
 struct Layout {
-  size_t a, scale, symbol, symbol32, tw, solutions, f, x, r, p, q, sw, spec, shat, partials, scal, macros,
+  size_t a, scale, scale32, symbol, symbol32, tw, solutions, f, x, r, p, q, sw, spec, shat, partials, scal, macros,
       cond, r64, d, aux, total;
 };
 
@@ -94,6 +94,7 @@ struct pgj_ctx {
   // workspace views
   double* a;
   double* scale;
+  float* scale32;      // FP32 contexts: (3, N) component-planar FP32 copy of scale (first direction)
   double* symbol;
   float* symbol32;
   void* tw;            // n complex twiddles: double2[n] then float2[n]
@@ -148,6 +149,8 @@ int launch_green_pass(pgj_ctx* c, int loads, int prec, const void* r, bool init,
 int launch_green_standalone(pgj_ctx* c, int loads, const double* r, double* z, cudaStream_t s);
 int launch_fz_fused(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s);
 int build_shat(pgj_ctx* c, cudaStream_t s);
+// FP32 contexts: scale32 = float(scale), component-planar (pgj_operator.cu)
+int launch_scale32(pgj_ctx* c, cudaStream_t s);
 // slab-fused iteration (pgj_slab.cu)
 enum SlabLaunch { kSlabUpdateL = 0, kSlabInitL = 1, kSlabSyncL = 2 };
 bool slab_fits(const pgj_ctx* c);

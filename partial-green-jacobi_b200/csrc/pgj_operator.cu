@@ -694,6 +694,21 @@ void element_diagonal(int n, double lam, double mu, double* ed) {
   for (int i = 0; i < 24; ++i) ed[i] *= vol8;
 }
 
+// s32[c][node] = float(s[3 node + c])
+__global__ void k_scale32(size_t N, const double* __restrict__ s, float* __restrict__ s32) {
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+    const double a = s[3 * i], b = s[3 * i + 1], c = s[3 * i + 2];
+    s32[i] = float(a);
+    s32[N + i] = float(b);
+    s32[2 * N + i] = float(c);
+  }
+}
+
+int launch_scale32(pgj_ctx* c, cudaStream_t s) {
+  k_scale32<<<296, 256, 0, s>>>(size_t(c->N), c->scale, c->scale32);
+  return check_launch();
+}
+
 int launch_scale(pgj_ctx* c, double alpha, cudaStream_t s) {
   const size_t count = 3 * size_t(c->N);
   if (alpha == 0.0) {

@@ -34,6 +34,7 @@ struct SlabArgs {
   void* u;                // (L,3N) U iterate (FP64 x, or the FP32 correction d)
   const double* r64;      // sync mode: FP64 true residual
   const double* scale;    // (3N) FP64 scale field s
+  const float* scale32;   // FP32 contexts: (3, N) component-planar FP32 copy of s
   void* spec;             // (L,3,n,n,nsp) complex T
   const void* tw;         // n complex T twiddles
   LoadScalars* scal;      // recurrence records
@@ -103,6 +104,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   const size_t off = size_t(load) * N3 + 3 * node0 + c;  // dof of node (0,0,z), component c
   T* r = reinterpret_cast<T*>(A.r) + off;
   const double* sc = A.scale + 3 * node0 + c;
+  const float* s32 = sizeof(T) == 4 ? A.scale32 + size_t(c) * nn * n + node0 : nullptr;  // coalesced
   T* packed = real_view<T>(b0);
   const int lpx = R64 ? kLine64 : n + 1;  // pitch of the packed x lines
   double acc[2] = {0.0, 0.0};
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
       const int i = i0 + j * nthr;
       if (i < nn) {
         const size_t k = 3 * size_t(i);
-        sv[j] = sc[k];
+        sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[k];
         if (MODE == kSlabUpdate) { pv[j] = pg[k]; qv[j] = qg[k]; rv[j] = r[k]; uv[j] = ug[k]; }
         else if (MODE == kSlabSync) rv[j] = T(r64[k]);
         else rv[j] = r[k];
@@ -354,6 +356,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
   const size_t off = size_t(load) * 3 * size_t(nn) * n + 3 * node0 + c;
   T* p = reinterpret_cast<T*>(A.p) + off;
   const double* sc = A.scale + 3 * node0 + c;
+  const float* s32 = sizeof(T) == 4 ? A.scale32 + size_t(c) * nn * n + node0 : nullptr;  // coalesced
   const T m = T(S.mean_z[c]);
   const T beta = T(S.beta);
   constexpr int UNR = 4;
@@ -365,7 +368,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
       const int i = i0 + j * nthr;
       if (i < nn) {
         const size_t k = 3 * size_t(i);
-        sv[j] = sc[k];
+        sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[k];
         pv[j] = A.init ? T(0) : p[k];
       }
     }
@@ -444,7 +447,7 @@ static SlabArgs slab_args(pgj_ctx* c, int loads, int prec) {
   A.div_ns = make_fastdiv(unsigned(c->ns));
   A.div_nh = make_fastdiv(unsigned(c->n / 2));
   A.p = c->p; A.q = c->q; A.r = c->r;
-  A.r64 = c->r64; A.scale = c->scale; A.spec = c->spec;
+  A.r64 = c->r64; A.scale = c->scale; A.scale32 = c->scale32; A.spec = c->spec;
   A.tw = prec == PGJ_FP32 ? static_cast<const void*>(static_cast<double2*>(c->tw) + c->n) : c->tw;
   A.scal = c->scal; A.out = c->scal_out; A.partials = c->partials;
   A.cap = 4000; A.rel_delta2 = c->rel_delta2; A.loads = loads;
