@@ -1,15 +1,16 @@
 // Matrix-free periodic HEX8 operator, right-hand side, stiffness-diagonal scaling and projection.
 //
 // The operator q = K(a) p is a z-streaming stencil: a block owns full x-rows of n nodes and
-// `ty` output node rows (plus one halo element row), and marches a chunk of z-planes. Each
-// thread owns one element column. Per element plane it reads the four nodes of its upper face
-// from shared memory (the plane is staged with cp.async while the previous plane computes),
+// `ty` output node rows (plus one halo element row), and marches a chunk of z-planes. Node planes
+// are staged in shared memory by bulk asynchronous copies (one row per copy, issued by the lanes
+// of warp 0, 2-4 plane buffers, mbarrier completion; cp.async when rows are not 16-byte aligned).
+// Each thread owns one element column. Per element plane it reads the four nodes of its upper face,
 // forms the 2D Hadamard face modes, combines them with the lower face modes kept in registers
-// (z-level), applies the modal element action, and splits the force modes into the parts that
-// belong to the lower and upper node planes. The lower plane is complete once the element
-// below it has been added; its y- and x-level transposes are exchanged through shared memory
-// in a fixed order, so the result is deterministic (no atomics, unlike the reference's
-// scatter in exp/asg_gpu_resident_20261103/scalar_fi.cu:14-36).
+// (z-level), applies the modal element action, and splits the lower face into its four corner
+// nodes: it keeps the (x, y) corner and hands the other three to their owners through a
+// double-buffered exchange array, so one block barrier per plane publishes them. Fixed summation
+// order: the result is deterministic (no atomics, unlike the reference's scatter in
+// exp/asg_gpu_resident_20261103/scalar_fi.cu:14-36).
 #include "pgj_internal.h"
 #include <cmath>
 #include <cstdlib>
@@ -32,6 +33,24 @@ template <> __device__ __forceinline__ void cp_async<float>(float* dst, const fl
 __device__ __forceinline__ void cp_commit() { asm volatile("cp.async.commit_group;\n" ::); }
 __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_group 0;\n" ::); }
 __device__ __forceinline__ void cp_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::); }
+
+// The rows of one plane issued by the lanes of one warp in parallel (lane r: rows r, r+32, ...):
+// lane 0 arms the mbarrier for all rows first. Called by all 32 lanes of the warp.
+template <typename T>
+__device__ __forceinline__ void tma_plane_warp(T* buf, const T* in, int pz, int y0, int rows, int n, uint64_t* bar,
+                                               int lane) {
+  const unsigned rowbytes = unsigned(3 * n * sizeof(T));
+  if (lane == 0) {
+    fence_proxy_async();
+    mbar_expect_tx(bar, rowbytes * rows);
+  }
+  __syncwarp();
+  for (int r = lane; r < rows; r += 32) {
+    int y = (y0 - 1 + r) % n;
+    if (y < 0) y += n;
+    tma_row(buf + r * 3 * n, in + (size_t(pz) * n + y) * size_t(3 * n), rowbytes, bar);
+  }
+}
 
 template <typename T>
 __device__ __forceinline__ void tma_plane(T* buf, const T* in, int pz, int y0, int rows, int n, uint64_t* bar) {
@@ -285,7 +304,7 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
       if (tid == 0 && A.err) atomicExch(A.err, 1);
       return;
     }
-    if (tma && tid == 0 && s + 1 + NS < nplanes) tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb]);
+    if (tma && tid < 32 && s + 1 + NS < nplanes) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid);
     if (++jb == NS) { jb = 0; jpar ^= 1u; }
     zr = zr + 1 == n ? 0 : zr + 1;
     if (s >= 1 && out_row) {
