@@ -242,6 +242,7 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   int jb = 1 % NS;
   unsigned jpar = 0u;
   int zr = (z0 + NS) % n;
+  const bool full_warp0 = nthr >= 32;
   const int tl = ty * n + (tx == 0 ? n - 1 : tx - 1);          // element to the left (periodic x)
   const int tb = (ty >= 1 ? ty - 1 : 0) * n + tx;              // element below
   const int tbl = (ty >= 1 ? ty - 1 : 0) * n + (tx == 0 ? n - 1 : tx - 1);
@@ -304,7 +305,15 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
       if (tid == 0 && A.err) atomicExch(A.err, 1);
       return;
     }
-    if (tma && tid < 32 && s + 1 + NS < nplanes) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid);
+    if (tma && s + 1 + NS < nplanes) {
+      // warp 0 refills (its lanes issue the rows in parallel); a block of fewer than 32 threads
+      // has no full warp, and thread 0 issues the rows alone
+      if (full_warp0) {
+        if (tid < 32) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid);
+      } else if (tid == 0) {
+        tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb]);
+      }
+    }
     if (++jb == NS) { jb = 0; jpar ^= 1u; }
     zr = zr + 1 == n ? 0 : zr + 1;
     if (s >= 1 && out_row) {
