@@ -192,6 +192,24 @@ class Server:
         self.peak_used = 0
         self.max_inflight = 0  # most requests on the device at once
 
+    def warm(self, requests) -> None:
+        """Create one worker (context, stream, solve graph) for every grid size and precision these
+        requests will use, outside any timed run."""
+        torch = _torch()
+        kinds = sorted({(self._n_of(r), self._precision_for(r)) for r in requests}
+                       | ({(self._n_of(r), "fp64") for r in requests} if self.precision == "mixed" else set()))
+        for n, prec in kinds:
+            w = self._worker_for(n, prec, 0)
+            if w is None:
+                continue
+            with torch.cuda.stream(w.stream):
+                a = torch.ones((n, n, n), dtype=torch.float64, device="cuda")
+                w.op.set_material(a)
+                w.op.set_alpha(0.5)
+                w.u0.zero_()
+                w.op.solve(self.macros, self.rtol, w.u0)  # homogeneous: certifies at once, builds the graphs
+        torch.cuda.synchronize()
+
     # ----------------------------------------------------------------------------- admission
     def _n_of(self, req) -> int:
         return int(req.n) if isinstance(req, Lineage) else int(req.a.shape[0])
