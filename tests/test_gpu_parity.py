@@ -569,3 +569,23 @@ def test_serving_mixed_falls_back_to_fp64_and_certifies(pkg):
     out = server.run([sv.Arrival(0.0, lin)], realtime=False)
     assert len(out) == 1 and server.fallbacks == 1
     assert out[0].precision == "fp64-fallback" and out[0].status == 0
+
+
+def test_n96_mixed_and_fp64_certify_and_agree(pkg):
+    """n = 96 (the mixed-refinement grid size): the mixed solve runs the generic fused kernels, the
+    FP64 solve the step-by-step kernels (its slab does not fit in shared memory); both certify and
+    C_H agrees to the mixed tolerance."""
+    n = 96
+    lam, mu = pkg.PAPER_MEDIUM
+    a = dev(pkg.baseline_design(n, seed=3, emin=1e-6))
+    out = {}
+    for prec in ("fp64", "mixed"):
+        op = pkg.Operator(n, 6, lam, mu, precision=prec)
+        op.set_material(a)
+        op.set_alpha(0.5)
+        assert op.fused_iteration == (prec == "mixed")
+        u = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")
+        infos, st = op.solve(np.eye(6), 1e-8, u)
+        assert st == 0 and all(i["relative_residual"] <= 1e-8 for i in infos), (prec, infos)
+        out[prec] = op.effective_tensor(u).cpu().numpy()
+    assert rel(out["mixed"], out["fp64"]) < 1e-7, rel(out["mixed"], out["fp64"])
