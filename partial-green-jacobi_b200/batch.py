@@ -10,7 +10,7 @@ form of the reference's per-design loop (``exp/asg_density_selector_20261105/run
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 import numpy as np
 
