@@ -238,10 +238,22 @@ class Server:
             self.used -= w.bytes
         if self.used + need > self.budget:
             return None
-        w = _Worker(n, prec, self.lam, self.mu)
+        w = self._new_worker(n, prec)
         self.workers.append(w)
         self.used += w.bytes
         return w
+
+    def _new_worker(self, n: int, prec: str) -> _Worker:
+        return _Worker(n, prec, self.lam, self.mu)
+
+    def _snapshot_iterate(self, w: _Worker):
+        """Copy of a worker's homogenization iterate, complete before the call returns."""
+        u = w.u0.clone()
+        _torch().cuda.current_stream().synchronize()
+        return u
+
+    def _drain(self) -> None:
+        _torch().cuda.synchronize()
 
     # ----------------------------------------------------------------------------- launch / finish
     def _launch(self, w: _Worker, job: _Job) -> None:
@@ -312,7 +324,6 @@ class Server:
     # ----------------------------------------------------------------------------- loop
     def run(self, arrivals: list[Arrival], realtime: bool = True, idle_sleep: float = 2e-4) -> list[StepResult]:
         """Serve `arrivals` (sorted or not). With realtime=False every request is ready at t=0."""
-        torch = _torch()
         pending = deque(sorted(arrivals, key=lambda a: a.t))
         ready: deque[_Job] = deque()
         inflight: list[_Worker] = []
@@ -361,8 +372,7 @@ class Server:
                         redo = _Job(req=job.req, ready=job.ready, lineage=job.lineage, step=job.step,
                                     precision="fp64", fallback=True)
                         if job.lineage is None:
-                            redo.u_start = w.u0.clone()
-                            torch.cuda.current_stream().synchronize()  # copy done before the redo's stream
+                            redo.u_start = self._snapshot_iterate(w)
                         ready.appendleft(redo)
                         continue
                     results.append(res)
@@ -380,7 +390,7 @@ class Server:
                     time.sleep(min(idle_sleep * 10, max(0.0, pending[0].t - (time.perf_counter() - t0))))
                 else:
                     time.sleep(idle_sleep)
-        torch.cuda.synchronize()
+        self._drain()
         return results
 
 
