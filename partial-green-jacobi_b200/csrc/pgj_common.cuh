@@ -105,6 +105,16 @@ template <typename C> __device__ __forceinline__ C cmulc(C a, C b) {
   C c; c.x = a.x * b.x + a.y * b.y; c.y = a.y * b.x - a.x * b.y; return c;
 }
 template <typename C> __device__ __forceinline__ C cconj(C a) { a.y = -a.y; return a; }
+// FP32 complex arithmetic as packed FP32 operations (two results per instruction on sm_100);
+// adds and subtracts round exactly like their scalar forms
+template <> __device__ __forceinline__ float2 cadd<float2>(float2 a, float2 b) { return __fadd2_rn(a, b); }
+template <> __device__ __forceinline__ float2 csub<float2>(float2 a, float2 b) {
+  return __fadd2_rn(a, make_float2(-b.x, -b.y));
+}
+template <> __device__ __forceinline__ float2 cmul<float2>(float2 a, float2 b) {
+  const float2 t = __fmul2_rn(make_float2(a.y, a.y), make_float2(b.y, b.x));    // (ay by, ay bx)
+  return __ffma2_rn(make_float2(a.x, a.x), b, make_float2(-t.x, t.y));         // (ax bx - ay by, ax by + ay bx)
+}
 // multiply by -i (forward) or +i (inverse)
 template <typename C> __device__ __forceinline__ C cmul_mi(C a, bool inv) {
   C c; if (inv) { c.x = -a.y; c.y = a.x; } else { c.x = a.y; c.y = -a.x; } return c;
