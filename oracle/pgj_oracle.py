@@ -545,6 +545,31 @@ def paper_physical(t, hs, beta=4.0, eta=0.5, emin=1e-9):
     return rho, beta * (1 - q * q) / den, emin + (1 - emin) * rho ** 3
 
 
+def paper_local_energy(u, n, lam, mu, objective="shear", iteration=0):
+    """Local objective density of the Study II objectives (``reproduction.py:153-164``).
+
+    ``u`` holds the six Voigt-load solutions. The hydrostatic solution is u0 + u1 + u2 by linearity.
+    Returns (local (N,), per-load energies (6, N)).
+    """
+    e = energies(u, affine(n, np.eye(6)), n, lam, mu)
+    if objective == "shear":
+        return -e[3:].sum(0), e
+    hydro = energies(u[:3].sum(0, keepdims=True), affine(n, [[1.0, 1.0, 1.0, 0.0, 0.0, 0.0]]), n, lam, mu)[0]
+    if objective == "bulk":
+        return -hydro, e
+    if objective == "auxetic":
+        return hydro - (1 + 0.8 ** iteration) * e[:3].sum(0), e
+    raise ValueError(objective)
+
+
+def paper_sensitivity(energy, ph, dp, hs, rmin, emin=1e-9):
+    """Filtered objective and volume sensitivities d/dx of mean(local * a) and of sum(rho)
+    (``reproduction.py:91-94``; the check of ``asg_sctop_reproduction_20261105/verify.py:60-61``)."""
+    n = ph.shape[0]
+    g = cone_filter(dp * (3 * (1 - emin) * ph * ph) * energy / hs, rmin) / n ** 3
+    return g, cone_filter(dp / hs, rmin)
+
+
 def paper_oc(x, energy, ph, dp, hs, rmin, volume, beta=4.0, eta=0.5, emin=1e-9, move=0.1,
              exponent=0.3, floor=0.001, max_steps=180):
     """Damped OC with MATLAB-style bisection stop (``reproduction.py:91-104``, ``outer.cu:29-39``).
@@ -552,9 +577,7 @@ def paper_oc(x, energy, ph, dp, hs, rmin, volume, beta=4.0, eta=0.5, emin=1e-9, 
     ``energy`` is the local objective density (negative for stiffness maximisation).
     Returns (new, steps, change).
     """
-    n = x.shape[0]
-    g = cone_filter(dp * (3 * (1 - emin) * ph * ph) * energy / hs, rmin) / n ** 3
-    dv = cone_filter(dp / hs, rmin)
+    g, dv = paper_sensitivity(energy, ph, dp, hs, rmin, emin)
     ratio = -g / dv
     lo, hi, flag, steps = 0.0, 1e9, 1.0, 0
     new = x.copy()
