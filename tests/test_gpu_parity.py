@@ -190,12 +190,14 @@ def test_six_load_homogenization_matches_oracle(pkg, oracle, n, emin, alpha):
     assert all(i["relative_residual"] <= 1e-8 for i in infos)
 
 
-def test_homogeneous_gives_c0_and_zero_iterations(pkg):
+@pytest.mark.parametrize("value,alpha", [(1.0, 0.5), (0.13, 1.0)])
+def test_homogeneous_gives_c0_and_zero_iterations(pkg, value, alpha):
+    """Compatible zero RHS: a constant field certifies at the zero start (verify.py:47-49, study.py:294-301)."""
     n = 8
     lam, mu = pkg.PAPER_MEDIUM
     op = pkg.Operator(n, 6, lam, mu)
-    op.set_material(torch.ones((n, n, n), dtype=torch.float64, device="cuda"))
-    op.set_alpha(0.5)
+    op.set_material(torch.full((n, n, n), value, dtype=torch.float64, device="cuda"))
+    op.set_alpha(alpha)
     u = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")
     infos, st = op.solve(np.eye(6), 1e-8, u)
     assert st == 0
@@ -203,7 +205,8 @@ def test_homogeneous_gives_c0_and_zero_iterations(pkg):
     C = op.effective_tensor(u).cpu().numpy()
     c0 = np.zeros((6, 6)); c0[:3, :3] = lam; c0[np.arange(3), np.arange(3)] += 2 * mu
     c0[np.arange(3, 6), np.arange(3, 6)] = mu
-    assert np.abs(C - c0).max() < 1e-11
+    assert all(i["converged"] for i in infos)
+    assert np.abs(C - value * c0).max() < 1e-11
 
 
 def test_serial_equals_parallel(pkg):
