@@ -126,8 +126,52 @@ __device__ __forceinline__ void stage_plane(T* buf, const T* in, int pz, int y0,
   cp_commit();
 }
 
+// Three displacement components of one node or mode. FP32 keeps (x, y) as one packed pair, so an
+// add or subtract of two triples is two instructions on sm_100 instead of three. A packed add
+// rounds like a scalar one, but the compiler no longer fuses a preceding product into it (as it
+// does in scalar code), so FP32 results differ from a scalar build in the last bits.
+template <typename T>
+struct Tri {
+  T x, y, z;
+  __device__ __forceinline__ T get(int c) const { return c == 0 ? x : (c == 1 ? y : z); }
+  static __device__ __forceinline__ Tri make(T a, T b, T c) { return Tri{a, b, c}; }
+  static __device__ __forceinline__ Tri load(const T* p) { return Tri{p[0], p[1], p[2]}; }
+  __device__ __forceinline__ void store(T* p) const { p[0] = x; p[1] = y; p[2] = z; }
+  friend __device__ __forceinline__ Tri operator+(Tri a, Tri b) { return Tri{a.x + b.x, a.y + b.y, a.z + b.z}; }
+  friend __device__ __forceinline__ Tri operator-(Tri a, Tri b) { return Tri{a.x - b.x, a.y - b.y, a.z - b.z}; }
+};
+template <>
+struct Tri<float> {
+  float2 xy;
+  float z;
+  __device__ __forceinline__ float get(int c) const { return c == 0 ? xy.x : (c == 1 ? xy.y : z); }
+  static __device__ __forceinline__ Tri make(float a, float b, float c) { return Tri{make_float2(a, b), c}; }
+  static __device__ __forceinline__ Tri load(const float* p) { return Tri{make_float2(p[0], p[1]), p[2]}; }
+  __device__ __forceinline__ void store(float* p) const { p[0] = xy.x; p[1] = xy.y; p[2] = z; }
+  friend __device__ __forceinline__ Tri operator+(Tri a, Tri b) { return Tri{__fadd2_rn(a.xy, b.xy), a.z + b.z}; }
+  friend __device__ __forceinline__ Tri operator-(Tri a, Tri b) {
+    return Tri{__fadd2_rn(a.xy, make_float2(-b.xy.x, -b.xy.y)), a.z - b.z};
+  }
+};
+
 // Read the 4 nodes of the face (x..x+1, row..row+1) from a staged plane and form the face modes
-// F[f][c], f = mx + 2 my: F[0] = sum, F[1] = x-difference, F[2] = y-difference, F[3] = both.
+// F[f], f = mx + 2 my: F[0] = sum, F[1] = x-difference, F[2] = y-difference, F[3] = both.
+template <typename T>
+__device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, Tri<T> (&F)[4], Tri<T>& own) {
+  const int xp = (x + 1 == n) ? 0 : x + 1;
+  const T* r0 = buf + row * 3 * n;
+  const T* r1 = r0 + 3 * n;
+  const Tri<T> u00 = Tri<T>::load(r0 + 3 * x), u10 = Tri<T>::load(r0 + 3 * xp);
+  const Tri<T> u01 = Tri<T>::load(r1 + 3 * x), u11 = Tri<T>::load(r1 + 3 * xp);
+  own = u00;
+  const Tri<T> sx0 = u10 + u00, dx0 = u10 - u00, sx1 = u11 + u01, dx1 = u11 - u01;
+  F[0] = sx1 + sx0;
+  F[1] = dx1 + dx0;
+  F[2] = sx1 - sx0;
+  F[3] = dx1 - dx0;
+}
+
+// The same face modes one component at a time (the FP64 loop).
 template <typename T>
 __device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, T (&F)[4][3], T (&own)[3]) {
   const int xp = (x + 1 == n) ? 0 : x + 1;
@@ -211,142 +255,281 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
     cp_wait_one();
     __syncthreads();
   }
-  T F0[4][3], own[3], dummy[3];
-  face_modes(bufs, ty, tx, n, F0, dummy);
-  if (tma) {
-    // buffer 0 is free once every thread has read plane 0
-    if (__syncthreads_or(bad)) {
-      if (tid == 0 && A.err) atomicExch(A.err, 1);
-      return;
-    }
-    if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0]);
-  }
-  T Up[4][3];
-#pragma unroll
-  for (int f = 0; f < 4; ++f)
-#pragma unroll
-    for (int c = 0; c < 3; ++c) Up[f][c] = T(0);
-#pragma unroll
-  for (int c = 0; c < 3; ++c) own[c] = T(0);
-
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  const double* aa = A.a;
-
-  // element densities are read one plane ahead so their latency overlaps the previous plane
-  const double* arow = aa + size_t(eyw) * n + tx;
-  const size_t aplane = size_t(n) * n;
-  int za = (z0 - 1 + n) % n;  // element plane of the next density read (wraps incrementally)
-  double a_next = __ldg(arow + size_t(za) * aplane);
-  // buffer / phase bookkeeping without divisions: plane j = s + 1 sits in buffer jb with mbarrier
-  // parity jpar; after the step's barrier that buffer takes plane s + 1 + NS (node plane zr)
-  int jb = 1 % NS;
-  unsigned jpar = 0u;
-  int zr = (z0 + NS) % n;
-  const bool full_warp0 = nthr >= 32;
-  const int tl = ty * n + (tx == 0 ? n - 1 : tx - 1);          // element to the left (periodic x)
-  const int tb = (ty >= 1 ? ty - 1 : 0) * n + tx;              // element below
-  const int tbl = (ty >= 1 ? ty - 1 : 0) * n + (tx == 0 ? n - 1 : tx - 1);
-  const int tme = ty * n + tx;
-  for (int s = 0; s <= zc; ++s) {
-    const int ez = z0 - 1 + s;           // element plane
-    const T ae = T(a_next);
-    if (s < zc) {
-      za = za + 1 == n ? 0 : za + 1;
-      a_next = __ldg(arow + size_t(za) * aplane);
-    }
-    T* cur = bufs + jb * planevals;
+  if constexpr (sizeof(T) == 4) {
+    // FP32: packed-pair arithmetic (Tri) and two z-steps per loop trip, which removes the copies of
+    // the carried face modes; 47 vs 51 us at n = 64, 6 loads. FP64 keeps the one-step form below:
+    // the same restructuring made it slower (64 vs 61 us).
+    // lower-face modes, upper-plane carry and own node value of the plane below, in two sets that
+    // swap roles every z-step (no copies at the loop edge)
+    Tri<T> FA[4], UA[4], ownA, FB[4], UB[4], ownB;
+    face_modes(bufs, ty, tx, n, FA, ownB);
     if (tma) {
-      bad = bad || !mbar_wait(&bars[jb], jpar);
-    } else {
-      cp_wait_all();
-      __syncthreads();
-      if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
+      // buffer 0 is free once every thread has read plane 0
+      if (__syncthreads_or(bad)) {
+        if (tid == 0 && A.err) atomicExch(A.err, 1);
+        return;
+      }
+      if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0]);
     }
+#pragma unroll
+    for (int f = 0; f < 4; ++f) UA[f] = Tri<T>::make(T(0), T(0), T(0));
+    ownA = Tri<T>::make(T(0), T(0), T(0));
 
-    T F1[4][3], own1[3];
-    face_modes(cur, ty, tx, n, F1, own1);
-    // element modes: z level
-    T Q[8][3];
+    const double* aa = A.a;
+
+    // element densities are read one plane ahead so their latency overlaps the previous plane
+    const double* arow = aa + size_t(eyw) * n + tx;
+    const size_t aplane = size_t(n) * n;
+    int za = (z0 - 1 + n) % n;  // element plane of the next density read (wraps incrementally)
+    double a_next = __ldg(arow + size_t(za) * aplane);
+    // buffer / phase bookkeeping without divisions: plane j = s + 1 sits in buffer jb with mbarrier
+    // parity jpar; after the step's barrier that buffer takes plane s + 1 + NS (node plane zr)
+    int jb = 1 % NS;
+    unsigned jpar = 0u;
+    int zr = (z0 + NS) % n;
+    const bool full_warp0 = nthr >= 32;
+    const int tl = ty * n + (tx == 0 ? n - 1 : tx - 1);          // element to the left (periodic x)
+    const int tb = (ty >= 1 ? ty - 1 : 0) * n + tx;              // element below
+    const int tbl = (ty >= 1 ? ty - 1 : 0) * n + (tx == 0 ? n - 1 : tx - 1);
+    const int tme = ty * n + tx;
+
+    // One element plane s: F0 / Up / own0 hold the lower face modes, the carry from the element
+    // below and the own node value of node plane ez; F1 / U / own1 receive those of the next plane.
+    // Returns false when a bounded wait gave up (the block then leaves).
+    auto step = [&](int s, const Tri<T> (&F0)[4], const Tri<T> (&Up)[4], const Tri<T>& own0, Tri<T> (&F1)[4],
+                    Tri<T> (&U)[4], Tri<T>& own1) -> bool {
+      const int ez = z0 - 1 + s;           // element plane
+      const T ae = T(a_next);
+      if (s < zc) {
+        za = za + 1 == n ? 0 : za + 1;
+        a_next = __ldg(arow + size_t(za) * aplane);
+      }
+      T* cur = bufs + jb * planevals;
+      if (tma) {
+        bad = bad || !mbar_wait(&bars[jb], jpar);
+      } else {
+        cp_wait_all();
+        __syncthreads();
+        if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
+      }
+
+      face_modes(cur, ty, tx, n, F1, own1);
+      // element modes: z level
+      T Q[8][3];
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const Tri<T> sum = F1[f] + F0[f], dif = F1[f] - F0[f];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { Q[f][c] = sum.get(c); Q[f + 4][c] = dif.get(c); }
+      }
+      T P[8][3];
+      element_modal<T>(Q, ae, A.kc, P);
+      // z-level transpose: U -> upper plane (ez+1), G -> lower plane (ez)
+      Tri<T> G[4];
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        const Tri<T> lo = Tri<T>::make(P[f][0], P[f][1], P[f][2]);
+        const Tri<T> hi = Tri<T>::make(P[f + 4][0], P[f + 4][1], P[f + 4][2]);
+        U[f] = lo + hi;
+        G[f] = (lo - hi) + Up[f];
+      }
+      // lower face of the element (node plane ez) as its four corner nodes: this thread keeps the
+      // (x, y) corner and hands (x+1, y), (x, y+1), (x+1, y+1) to their owners through shared memory
+      Tri<T> c00;
+      T* xb = xch + (s & 1) * xsz;
+      if (s >= 1) {
+        const Tri<T> ly0 = G[0] - G[2], ly1 = G[1] - G[3];
+        const Tri<T> uy0 = G[0] + G[2], uy1 = G[1] + G[3];
+        c00 = ly0 - ly1;
+        (ly0 + ly1).store(xb + (0 * nt + tme) * 3);
+        (uy0 - uy1).store(xb + (1 * nt + tme) * 3);
+        (uy0 + uy1).store(xb + (2 * nt + tme) * 3);
+      }
+      // one barrier per step: corners published, plane jb fully read, timeouts agreed on
+      if (__syncthreads_or(bad)) {
+        if (tid == 0 && A.err) atomicExch(A.err, 1);
+        return false;
+      }
+      if (tma && s + 1 + NS < nplanes) {
+        // warp 0 refills (its lanes issue the rows in parallel); a block of fewer than 32 threads
+        // has no full warp, and thread 0 issues the rows alone
+        if (full_warp0) {
+          if (tid < 32) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid);
+        } else if (tid == 0) {
+          tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb]);
+        }
+      }
+      if (++jb == NS) { jb = 0; jpar ^= 1u; }
+      zr = zr + 1 == n ? 0 : zr + 1;
+      if (s >= 1 && out_row) {
+        const Tri<T> qx = ((c00 + Tri<T>::load(xb + (0 * nt + tl) * 3)) + Tri<T>::load(xb + (1 * nt + tb) * 3)) +
+                          Tri<T>::load(xb + (2 * nt + tbl) * 3);
+        const size_t node = (size_t(ez) * n + ey) * n + tx;
+        T* o = out + 3 * node;
+        if (MODE == kResidual) {
+          const double* fl = A.f + size_t(load) * 3 * N + 3 * node;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const double rv = fl[c] - double(qx.get(c));
+            o[c] = T(rv);
+            acc[0] += rv * rv;
+            acc[1 + c] += rv;
+          }
+        } else {
+          qx.store(o);
+          if (MODE == kPCG) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[0] += double(own0.get(c)) * double(qx.get(c));
+          }
+        }
+      }
+      return true;
+    };
+    // two steps per trip with the sets swapped (the carries stay where they were written)
+    for (int s = 0; s <= zc; s += 2) {
+      if (!step(s, FA, UA, ownA, FB, UB, ownB)) return;
+      if (s + 1 > zc) break;
+      if (!step(s + 1, FB, UB, ownB, FA, UA, ownA)) return;
+    }
+  } else {
+    T F0[4][3], own[3], dummy[3];
+    face_modes(bufs, ty, tx, n, F0, dummy);
+    if (tma) {
+      // buffer 0 is free once every thread has read plane 0
+      if (__syncthreads_or(bad)) {
+        if (tid == 0 && A.err) atomicExch(A.err, 1);
+        return;
+      }
+      if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0]);
+    }
+    T Up[4][3];
 #pragma unroll
     for (int f = 0; f < 4; ++f)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        Q[f][c] = F1[f][c] + F0[f][c];
-        Q[f + 4][c] = F1[f][c] - F0[f][c];
-      }
-    T P[8][3];
-    element_modal<T>(Q, ae, A.kc, P);
-    // z-level transpose: U -> upper plane (ez+1), G -> lower plane (ez)
-    T U[4][3], G[4][3];
+      for (int c = 0; c < 3; ++c) Up[f][c] = T(0);
 #pragma unroll
-    for (int f = 0; f < 4; ++f)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        U[f][c] = P[f][c] + P[f + 4][c];
-        G[f][c] = (P[f][c] - P[f + 4][c]) + Up[f][c];
+    for (int c = 0; c < 3; ++c) own[c] = T(0);
+
+    const double* aa = A.a;
+
+    // element densities are read one plane ahead so their latency overlaps the previous plane
+    const double* arow = aa + size_t(eyw) * n + tx;
+    const size_t aplane = size_t(n) * n;
+    int za = (z0 - 1 + n) % n;  // element plane of the next density read (wraps incrementally)
+    double a_next = __ldg(arow + size_t(za) * aplane);
+    // buffer / phase bookkeeping without divisions: plane j = s + 1 sits in buffer jb with mbarrier
+    // parity jpar; after the step's barrier that buffer takes plane s + 1 + NS (node plane zr)
+    int jb = 1 % NS;
+    unsigned jpar = 0u;
+    int zr = (z0 + NS) % n;
+    const bool full_warp0 = nthr >= 32;
+    const int tl = ty * n + (tx == 0 ? n - 1 : tx - 1);          // element to the left (periodic x)
+    const int tb = (ty >= 1 ? ty - 1 : 0) * n + tx;              // element below
+    const int tbl = (ty >= 1 ? ty - 1 : 0) * n + (tx == 0 ? n - 1 : tx - 1);
+    const int tme = ty * n + tx;
+    for (int s = 0; s <= zc; ++s) {
+      const int ez = z0 - 1 + s;           // element plane
+      const T ae = T(a_next);
+      if (s < zc) {
+        za = za + 1 == n ? 0 : za + 1;
+        a_next = __ldg(arow + size_t(za) * aplane);
       }
-    // lower face of the element (node plane ez) as its four corner nodes: this thread keeps the
-    // (x, y) corner and hands (x+1, y), (x, y+1), (x+1, y+1) to their owners through shared memory
-    T c00[3];
-    T* xb = xch + (s & 1) * xsz;
-    if (s >= 1) {
-#pragma unroll
-      for (int c = 0; c < 3; ++c) {
-        const T ly0 = G[0][c] - G[2][c], ly1 = G[1][c] - G[3][c];
-        const T uy0 = G[0][c] + G[2][c], uy1 = G[1][c] + G[3][c];
-        c00[c] = ly0 - ly1;
-        xb[(0 * nt + tme) * 3 + c] = ly0 + ly1;
-        xb[(1 * nt + tme) * 3 + c] = uy0 - uy1;
-        xb[(2 * nt + tme) * 3 + c] = uy0 + uy1;
+      T* cur = bufs + jb * planevals;
+      if (tma) {
+        bad = bad || !mbar_wait(&bars[jb], jpar);
+      } else {
+        cp_wait_all();
+        __syncthreads();
+        if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
       }
-    }
-    // one barrier per step: corners published, plane jb fully read, timeouts agreed on
-    if (__syncthreads_or(bad)) {
-      if (tid == 0 && A.err) atomicExch(A.err, 1);
-      return;
-    }
-    if (tma && s + 1 + NS < nplanes) {
-      // warp 0 refills (its lanes issue the rows in parallel); a block of fewer than 32 threads
-      // has no full warp, and thread 0 issues the rows alone
-      if (full_warp0) {
-        if (tid < 32) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid);
-      } else if (tid == 0) {
-        tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb]);
-      }
-    }
-    if (++jb == NS) { jb = 0; jpar ^= 1u; }
-    zr = zr + 1 == n ? 0 : zr + 1;
-    if (s >= 1 && out_row) {
-      T qx[3];
+
+      T F1[4][3], own1[3];
+      face_modes(cur, ty, tx, n, F1, own1);
+      // element modes: z level
+      T Q[8][3];
 #pragma unroll
-      for (int c = 0; c < 3; ++c)
-        qx[c] = ((c00[c] + xb[(0 * nt + tl) * 3 + c]) + xb[(1 * nt + tb) * 3 + c]) + xb[(2 * nt + tbl) * 3 + c];
-      const size_t node = (size_t(ez) * n + ey) * n + tx;
-      T* o = out + 3 * node;
-      if (MODE == kResidual) {
-        const double* fl = A.f + size_t(load) * 3 * N + 3 * node;
+      for (int f = 0; f < 4; ++f)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const double rv = fl[c] - double(qx[c]);
-          o[c] = T(rv);
-          acc[0] += rv * rv;
-          acc[1 + c] += rv;
+          Q[f][c] = F1[f][c] + F0[f][c];
+          Q[f + 4][c] = F1[f][c] - F0[f][c];
         }
-      } else {
+      T P[8][3];
+      element_modal<T>(Q, ae, A.kc, P);
+      // z-level transpose: U -> upper plane (ez+1), G -> lower plane (ez)
+      T U[4][3], G[4][3];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) o[c] = qx[c];
-        if (MODE == kPCG) {
+      for (int f = 0; f < 4; ++f)
 #pragma unroll
-          for (int c = 0; c < 3; ++c) acc[0] += double(own[c]) * double(qx[c]);
+        for (int c = 0; c < 3; ++c) {
+          U[f][c] = P[f][c] + P[f + 4][c];
+          G[f][c] = (P[f][c] - P[f + 4][c]) + Up[f][c];
+        }
+      // lower face of the element (node plane ez) as its four corner nodes: this thread keeps the
+      // (x, y) corner and hands (x+1, y), (x, y+1), (x+1, y+1) to their owners through shared memory
+      T c00[3];
+      T* xb = xch + (s & 1) * xsz;
+      if (s >= 1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+          const T ly0 = G[0][c] - G[2][c], ly1 = G[1][c] - G[3][c];
+          const T uy0 = G[0][c] + G[2][c], uy1 = G[1][c] + G[3][c];
+          c00[c] = ly0 - ly1;
+          xb[(0 * nt + tme) * 3 + c] = ly0 + ly1;
+          xb[(1 * nt + tme) * 3 + c] = uy0 - uy1;
+          xb[(2 * nt + tme) * 3 + c] = uy0 + uy1;
         }
       }
+      // one barrier per step: corners published, plane jb fully read, timeouts agreed on
+      if (__syncthreads_or(bad)) {
+        if (tid == 0 && A.err) atomicExch(A.err, 1);
+        return;
+      }
+      if (tma && s + 1 + NS < nplanes) {
+        // warp 0 refills (its lanes issue the rows in parallel); a block of fewer than 32 threads
+        // has no full warp, and thread 0 issues the rows alone
+        if (full_warp0) {
+          if (tid < 32) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid);
+        } else if (tid == 0) {
+          tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb]);
+        }
+      }
+      if (++jb == NS) { jb = 0; jpar ^= 1u; }
+      zr = zr + 1 == n ? 0 : zr + 1;
+      if (s >= 1 && out_row) {
+        T qx[3];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+          qx[c] = ((c00[c] + xb[(0 * nt + tl) * 3 + c]) + xb[(1 * nt + tb) * 3 + c]) + xb[(2 * nt + tbl) * 3 + c];
+        const size_t node = (size_t(ez) * n + ey) * n + tx;
+        T* o = out + 3 * node;
+        if (MODE == kResidual) {
+          const double* fl = A.f + size_t(load) * 3 * N + 3 * node;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const double rv = fl[c] - double(qx[c]);
+            o[c] = T(rv);
+            acc[0] += rv * rv;
+            acc[1 + c] += rv;
+          }
+        } else {
+#pragma unroll
+          for (int c = 0; c < 3; ++c) o[c] = qx[c];
+          if (MODE == kPCG) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[0] += double(own[c]) * double(qx[c]);
+          }
+        }
+      }
+#pragma unroll
+      for (int f = 0; f < 4; ++f)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) { F0[f][c] = F1[f][c]; Up[f][c] = U[f][c]; }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) own[c] = own1[c];
     }
-#pragma unroll
-    for (int f = 0; f < 4; ++f)
-#pragma unroll
-      for (int c = 0; c < 3; ++c) { F0[f][c] = F1[f][c]; Up[f][c] = U[f][c]; }
-#pragma unroll
-    for (int c = 0; c < 3; ++c) own[c] = own1[c];
+
   }
 
   if (MODE == kPlain) return;
