@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
 // kz = t + 8 k1. The inverse runs the same steps backwards. A warp owns four kx columns at one ky
 // (all three components); warps never wait on each other, so the only block barrier is the final
 // reduction. Same results as k_fz in fused mode (rz, beta and mean(s.w) by Parseval).
-constexpr int kFz64Line = 76;                 // complex slots per line (8 rows of 9, padded)
+constexpr int kFz64Line = 72;                 // complex slots per line (8 rows of 9; conflict-free, as kLine64)
 
 // The FI symbol at (kx, ky, kz) from the per-axis factors (m, v, d) of each wavenumber, the same
 // algebra as k_symbol: t = h^3 prod m, trace = t sum (d + v^2), inv_i = 1/(mu trace + (lam+mu) t d_i),

@@ -367,6 +367,8 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
                           Tri<T>::load(xb + (2 * nt + tbl) * 3);
         const size_t node = (size_t(ez) * n + ey) * n + tx;
         T* o = out + 3 * node;
+        // FP32 never runs the residual mode (the host rejects it); the branch is kept because the
+        // build without it allocates registers differently and measured 0.6 us slower
         if (MODE == kResidual) {
           const double* fl = A.f + size_t(load) * 3 * N + 3 * node;
 #pragma unroll

@@ -55,11 +55,14 @@ template <typename T>
 __device__ __forceinline__ T* real_view(cplx<T>* b) { return reinterpret_cast<T*>(b); }
 
 // n = 64: a 64-point line as an 8 x 8 four-step transform held by 8 lanes (lane t holds points
-// t + 8b), with the transpose through the line's own shared-memory region L (rows of 9, 76 slots).
+// t + 8b), with the transpose through the line's own shared-memory region L (rows of 9, 72 slots).
 // Forward from registers v[b] = x[t + 8b]: on return v[k1] = X[t + 8 k1]. Inverse from
 // v[k1] = X[t + 8 k1]: on return v[b] = x[t + 8 b] (unnormalised). The caller's eight lanes of the
 // line must be converged; L must not be read by other lanes meanwhile.
-constexpr int kLine64 = 76;
+// 72 slots: two lines that share a half-warp (FP32 complex values are 8 bytes, 16 lanes per
+// shared-memory pass) then sit 16 banks apart, so both the row and the column accesses of the
+// transpose are free of bank conflicts.
+constexpr int kLine64 = 72;
 template <typename T>
 __device__ __forceinline__ void line64(cplx<T> (&v)[8], cplx<T>* L, int t, const cplx<T>* __restrict__ tw, bool inv) {
   using C = cplx<T>;
@@ -84,7 +87,7 @@ __device__ __forceinline__ void line64(cplx<T> (&v)[8], cplx<T>* L, int t, const
 // W4: blocks of at most 288 threads, four resident per SM (56 registers); otherwise up to 512
 // threads, two per SM.
 // R64 (n = 64, 288 threads): x and y lines as register four-step transforms (line64); shared
-// memory holds 36 lines of 76 complex values (packed x lines, then per-warp transpose space) and
+// memory holds 36 lines of 72 complex values (packed x lines, then per-warp transpose space) and
 // the n x nsp half-spectrum rows.
 template <typename T, typename U, int MODE, bool W4, bool R64>
 __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabArgs A) {
