@@ -26,6 +26,8 @@ follows:
   ``exp/asg_gpu_resident_20261103/outer.py:12-59``, ``exp/asg_gpu_resident_20261103/outer.cu:7-37``
 * Study II cone filter / projection / OC ......... ``exp/asg_sctop_reproduction_20261105/reproduction.py:38-118``,
   ``exp/asg_sctop_reproduction_20261105/outer.cu:8-39``
+* alpha selectors (contrast, gray, compact8) ...... ``exp/asg_density_selector_20261105/run.py:27-43,53-67``,
+  ``solver/experiments/global_alpha_compact_law/law.py:10-19``
 
 Layouts follow the reference: a DOF vector is (L, 3N) float64, node-major with the xyz
 components interleaved, nodes in grid order (z, y, x); a scalar field is (n, n, n) in
@@ -598,3 +600,58 @@ def paper_oc(x, energy, ph, dp, hs, rmin, volume, beta=4.0, eta=0.5, emin=1e-9, 
         steps += 1
         flag = 1.0 if ((hi - lo) / (hi + lo) > 1e-4 and hi > 1e-40) else 0.0
     return new, steps, float(np.abs(new - x).max())
+
+
+# ----------------------------------------------------------------------------- alpha selectors
+def law_features(a: np.ndarray) -> np.ndarray:
+    """(area, jump, contrast, complexity) in FP32 (``solver/experiments/global_alpha_compact_law/law.py:10-19``)."""
+    ell = np.log(a.astype(np.float32))
+    lo, hi = ell.min(), ell.max()
+    span = np.float32(hi - lo)
+    q = (ell - lo) / max(span, np.float32(1e-12))
+    s1 = s2 = act = np.float32(0)
+    for axis in range(3):
+        d = np.abs(np.roll(q, -1, axis) - q)
+        s1 = s1 + d.mean(dtype=np.float32)
+        s2 = s2 + (d * d).mean(dtype=np.float32)
+        act = act + (d > 1e-6).astype(np.float32).mean(dtype=np.float32)
+    area = act / np.float32(3)
+    jump = s2 / max(s1, np.float32(1e-20))
+    return np.array([area, jump, span / np.float32(np.log(10000.0)), area * a.shape[0]], dtype=np.float32)
+
+
+def compact8_alpha(a: np.ndarray, quantize: bool = False) -> float:
+    """Compact law with exponent 8 and the 0.375 cut-off (``asg_density_selector_20261105/run.py:60-66``)."""
+    area, jump, contrast, complexity = (float(v) for v in law_features(a))
+    if not (complexity > 1e-12 and contrast > 1e-12):
+        return 0.0
+    v = 1.0 - 0.75 * np.sqrt(max(area * jump, 0.0)) / np.sqrt(max(contrast, 1e-30)) - (2.5 / max(complexity, 1e-30)) ** 8
+    v = min(1.0, max(0.0, v))
+    v = 0.0 if v < 0.375 else v
+    return float(np.floor(16 * v + 0.5) / 16) if quantize else v
+
+
+def _contrast_base(a, anchors):
+    s = min(9.0, max(0.0, float(np.log10(a.max() / a.min()))))
+    b4, b6, b9 = anchors
+    if s < 4:
+        return s, b4 * s / 4
+    if s < 6:
+        return s, b4 + (b6 - b4) * (s - 4) / 2
+    return s, b6 + (b9 - b6) * (s - 6) / 3
+
+
+def contrast_alpha(a: np.ndarray, anchors=(0.5625, 0.6875, 0.8125)) -> float:
+    """Contrast model rounded to sixteenths (``asg_density_selector_20261105/run.py:27-33``)."""
+    s, base = _contrast_base(a, anchors)
+    return float(np.floor(min(1.0, max(0.0, base)) * 16 + 0.5) / 16) if s > 1e-12 else 0.0
+
+
+def gray_alpha(a: np.ndarray, rho: np.ndarray, anchors=(0.5625, 0.75, 0.8125), gamma=0.075,
+               g_ref=0.3739899920170806) -> float:
+    """Contrast model shifted by the grayness of rho (``asg_density_selector_20261105/run.py:36-43``)."""
+    s, base = _contrast_base(a, anchors)
+    v = rho.mean()
+    g = min(1.0, max(0.0, float((v - (rho * rho).mean()) / (v * (1 - v) + 1e-12))))
+    value = base + gamma * (g_ref - g)
+    return float(np.floor(min(1.0, max(0.0, value)) * 16 + 0.5) / 16) if s > 1e-12 else 0.0

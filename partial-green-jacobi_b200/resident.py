@@ -10,8 +10,9 @@ These keep the call surface of the reference drivers (``examples/shear_design.py
 * ``SelectorResident``  ~ ``exp/asg_density_selector_20261105/run.py:46-77`` (choose + build_scale)
 
 Every numerical step runs in libpgj (hand-written sm_100a kernels) through its C ABI; PyTorch only
-provides device memory and the current stream. Device buffers are owned here (torch tensors) and
-lent to the library by pointer.
+provides device memory and the current stream, except the alpha selectors of ``SelectorResident``
+(one scalar per design from a few reductions over the density, ``selectors.py``). Device buffers
+are owned here (torch tensors) and lent to the library by pointer.
 """
 from __future__ import annotations
 
@@ -20,7 +21,7 @@ import math
 
 import numpy as np
 
-from . import _lib
+from . import _lib, selectors
 from .outer import PaperOuter, ResidentOuter
 
 STUDY1_MEDIUM = (4.0 / 3.0, 1.0)
@@ -364,16 +365,19 @@ class PaperResident(Resident):
 
 
 class SelectorResident(PaperResident):
-    """``choose`` (alpha) + ``build_scale`` (D^-alpha/2) as separate steps (run.py:46-77)."""
+    """``choose`` (alpha) + ``build_scale`` (D^-alpha/2) as separate steps (run.py:46-77).
+
+    Methods: green, gj, eta (lookup by Emin), contrast, gray, compact8, compact8q, or a number.
+    The selectors are small reductions over the density on the device (``selectors.py``).
+    """
 
     def __init__(self, *args, **kwargs):
         super().__init__(*args, **kwargs)
         emin = self.outer.emin
         self.eta_value = ETA_ANCHORS[min(ETA_ANCHORS, key=lambda k: abs(math.log10(k) - math.log10(emin)))]
-        self.contrast_anchors = (0.5625, 0.6875, 0.8125)
+        self.contrast_anchors = selectors.CONTRAST_ANCHORS
 
     def choose(self, method):
-        torch = _torch()
         a = self.op._material_field
         if method == "green":
             self.alpha.zero_()
@@ -382,12 +386,11 @@ class SelectorResident(PaperResident):
         elif method == "eta":
             self.alpha.fill_(self.eta_value)
         elif method == "contrast":
-            lo, hi = torch.aminmax(a)
-            s = torch.log10(hi / lo).clamp(0.0, 9.0)
-            b4, b6, b9 = self.contrast_anchors
-            value = torch.where(s < 4, b4 * s / 4, torch.where(s < 6, b4 + (b6 - b4) * (s - 4) / 2,
-                                                                b6 + (b9 - b6) * (s - 6) / 3))
-            self.alpha.copy_(torch.where(s > 1e-12, (value.clamp(0, 1) * 16 + 0.5).floor() / 16, 0.0))
+            self.alpha.copy_(selectors.contrast_alpha(a, self.contrast_anchors))
+        elif method == "gray":
+            self.alpha.copy_(selectors.gray_alpha(a, self.outer.ph))
+        elif method in ("compact8", "compact8q"):
+            self.alpha.copy_(selectors.compact8_alpha(a, quantize=method == "compact8q"))
         else:
             try:
                 self.alpha.fill_(float(method))
