@@ -10,9 +10,9 @@ from .resident import (Backend, Operator, PaperBackend, PaperResident, Resident,
 from .outer import PaperOuter, ResidentOuter, cone_stencil, gaussian_weights
 from .designs import baseline_density, baseline_design, simp, study1_state0
 from .batch import Batch, Request, Result
-from . import selectors, serve
+from . import replay_state, selectors, serve
 
 __all__ = ["Backend", "Operator", "PaperBackend", "PaperResident", "Resident", "SelectorResident", "PaperOuter",
            "ResidentOuter", "cone_stencil", "gaussian_weights", "baseline_density", "baseline_design", "simp",
-           "study1_state0", "Batch", "Request", "Result", "selectors", "serve", "ETA_ANCHORS", "PAPER_MEDIUM",
+           "study1_state0", "Batch", "Request", "Result", "replay_state", "selectors", "serve", "ETA_ANCHORS", "PAPER_MEDIUM",
            "STUDY1_MEDIUM", "_lib"]
