@@ -8,11 +8,11 @@ from . import _lib
 from .resident import (Backend, Operator, PaperBackend, PaperResident, Resident, SelectorResident, ETA_ANCHORS,
                        PAPER_MEDIUM, STUDY1_MEDIUM)
 from .outer import PaperOuter, ResidentOuter, cone_stencil, gaussian_weights
-from .designs import baseline_density, baseline_design, simp, study1_state0
+from .designs import baseline_density, baseline_design, simp, study1_initial, study1_state0
 from .batch import Batch, Request, Result
-from . import replay_state, selectors, serve
+from . import replay_state, selectors, serve, shear_design
 
 __all__ = ["Backend", "Operator", "PaperBackend", "PaperResident", "Resident", "SelectorResident", "PaperOuter",
            "ResidentOuter", "cone_stencil", "gaussian_weights", "baseline_density", "baseline_design", "simp",
-           "study1_state0", "Batch", "Request", "Result", "replay_state", "selectors", "serve", "ETA_ANCHORS", "PAPER_MEDIUM",
-           "STUDY1_MEDIUM", "_lib"]
+           "study1_initial", "study1_state0", "Batch", "Request", "Result", "replay_state", "selectors", "serve",
+           "shear_design", "ETA_ANCHORS", "PAPER_MEDIUM", "STUDY1_MEDIUM", "_lib"]

@@ -3,8 +3,8 @@
 ``baseline_density``: N(0,1) noise -> periodic Gaussian filter (sigma = n/16 cells) -> smooth
 threshold at the (1 - vf) quantile, rho = logistic((f - q_{1-vf}) / (width * std f)), width 0.1.
 ``simp``: E = Emin + rho^p (E0 - Emin), E0 = 1, p = 3.
-``study1_state0``: the reference's Study I state 0, material(physical(initial(n, seed), 1)[0])
-(exp/asg_topopt_20261103/study.py:61-88).
+``study1_initial`` / ``study1_state0``: the reference's Study I initial design and its state 0,
+material(physical(initial(n, seed), 1)[0]) (exp/asg_topopt_20261103/study.py:61-88).
 """
 from __future__ import annotations
 
@@ -38,7 +38,10 @@ def _study1_physical(x, beta):
     return (np.tanh(beta / 2) + np.tanh(beta * (t - 0.5))) / den
 
 
-def study1_state0(n: int, seed: int = 20261104) -> np.ndarray:
+def study1_initial(n: int, seed: int = 20261104) -> np.ndarray:
+    """Study I initial design density: 12 random periodic cosine modes (std 0.12) around 0.3,
+    shifted by 50 bisections so that the beta = 1 physical density has volume 0.3
+    (exp/asg_topopt_20261103/study.py:75-88)."""
     rng = np.random.default_rng(seed)
     z, y, x = np.meshgrid(*([(np.arange(n) + 0.5) / n] * 3), indexing="ij")
     field = np.zeros((n, n, n))
@@ -57,5 +60,9 @@ def study1_state0(n: int, seed: int = 20261104) -> np.ndarray:
             hi = shift
         else:
             lo = shift
-    ph = _study1_physical(cand, 1.0)
+    return cand
+
+
+def study1_state0(n: int, seed: int = 20261104) -> np.ndarray:
+    ph = _study1_physical(study1_initial(n, seed), 1.0)
     return 1e-4 + (1 - 1e-4) * ph ** 3

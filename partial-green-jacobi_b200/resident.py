@@ -298,6 +298,9 @@ class Resident:
             alpha = 0.0
         elif method == "gj":
             alpha = 1.0
+        elif method == "compact8":
+            # compact law on the density field (exp/asg_gpu_resident_20261103/resident.py:163-168)
+            alpha = float(selectors.compact8_alpha(self.op._material_field))
         else:
             try:
                 alpha = float(method)
