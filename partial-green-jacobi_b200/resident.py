@@ -11,8 +11,8 @@ These keep the call surface of the reference drivers (``examples/shear_design.py
 
 Every numerical step runs in libpgj (hand-written sm_100a kernels) through its C ABI; PyTorch only
 provides device memory and the current stream, except the alpha selectors of ``SelectorResident``
-(one scalar per design from a few reductions over the density, ``selectors.py``). Device buffers
-are owned here (torch tensors) and lent to the library by pointer.
+(one scalar per design from a few reductions over the density, ``alpha_selectors.py``). Device
+buffers are owned here (torch tensors) and lent to the library by pointer.
 """
 from __future__ import annotations
 
@@ -21,7 +21,7 @@ import math
 
 import numpy as np
 
-from . import _lib, selectors
+from . import _lib, alpha_selectors as selectors
 from .outer import PaperOuter, ResidentOuter
 
 STUDY1_MEDIUM = (4.0 / 3.0, 1.0)
@@ -371,7 +371,7 @@ class SelectorResident(PaperResident):
     """``choose`` (alpha) + ``build_scale`` (D^-alpha/2) as separate steps (run.py:46-77).
 
     Methods: green, gj, eta (lookup by Emin), contrast, gray, compact8, compact8q, or a number.
-    The selectors are small reductions over the density on the device (``selectors.py``).
+    The selectors are small reductions over the density on the device (``alpha_selectors.py``).
     """
 
     def __init__(self, *args, **kwargs):

@@ -45,3 +45,14 @@ def test_product_path_has_no_oracle_import():
     for p in pkg_dir.glob("*.py"):
         assert "pgj_oracle" not in p.read_text(), p
         assert "oracle" not in re.findall(r"^\s*(?:from|import)\s+(\S+)", p.read_text(), flags=re.M), p
+
+
+def test_package_modules_do_not_shadow_the_standard_library():
+    """Scripts run from the package directory (build.py, profile_iteration.py, the drivers) put it
+    first on sys.path, so no module there may share a standard-library name."""
+    import sys
+    from pathlib import Path
+
+    pkg_dir = Path(__file__).resolve().parents[1] / "partial-green-jacobi_b200"
+    names = {p.stem for p in pkg_dir.glob("*.py")}
+    assert not names & set(sys.stdlib_module_names), names & set(sys.stdlib_module_names)

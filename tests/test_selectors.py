@@ -27,7 +27,7 @@ def test_oracle_law_features_match_reference(oracle, golden):
 
 
 def test_selectors_match_reference_and_oracle_on_cpu(pkg, oracle, golden):
-    sel = pkg.selectors
+    sel = pkg.alpha_selectors
     for name, g in golden.items():
         a = torch.tensor(g["a"], dtype=torch.float64)
         assert np.allclose(sel.law_features(a).numpy(), g["features"], rtol=1e-5, atol=1e-7), name
@@ -40,7 +40,7 @@ def test_selectors_match_reference_and_oracle_on_cpu(pkg, oracle, golden):
 
 
 def test_selector_edge_cases(pkg, golden):
-    sel = pkg.selectors
+    sel = pkg.alpha_selectors
     flat = torch.tensor(golden["homogeneous"]["a"])
     # a homogeneous field: no contrast, every selector gives the plain Green preconditioner
     for value in (sel.compact8_alpha(flat), sel.compact8_alpha(flat, quantize=True), sel.contrast_alpha(flat),
