@@ -63,8 +63,21 @@ class ResidentOuter:
         for name in ["x", "ph", "dp", "a", "energy", "new", "t"]:
             setattr(self, name, torch.empty(shape, device="cuda", dtype=torch.float64))
         self.scratch = torch.empty(4 * n ** 3 + 512, device="cuda", dtype=torch.float64)
+        self.scratch[4 * n ** 3:4 * n ** 3 + 8].zero_()  # bisection bounds and the change record
         self.beta = 1.0
-        self.change = 0.0
+
+    @property
+    def change(self):
+        """max |new - x| of the last OC update: a (1,) device tensor, updated in place like the
+        reference's ``outer.change`` (exp/asg_gpu_resident_20261103/outer.py:23,44)."""
+        N = self.n ** 3
+        return self.scratch[4 * N + 4:4 * N + 5]
+
+    @property
+    def bounds(self):
+        """(lo, hi) of the last multiplier bisection, on the device (outer.py:22,38)."""
+        N = self.n ** 3
+        return self.scratch[4 * N:4 * N + 2]
 
     def capture(self):
         return None
@@ -85,11 +98,10 @@ class ResidentOuter:
 
     def step(self, energy):
         self.energy.copy_(energy)
-        ch = C.c_double()
+        ch = C.c_double()  # asking for the host copy makes the call return once the update is done
         _lib.check(_lib.lib().pgj_study1_oc(self.n, _p(self.weights), self.radius, _p(self.x), _p(self.ph),
                                             _p(self.dp), _p(self.energy), self.beta, self.volume, self.move,
                                             _p(self.new), _p(self.scratch), C.byref(ch), _sp()), "pgj_study1_oc")
-        self.change = ch.value
 
     def advance(self):
         self.x.copy_(self.new)
@@ -106,9 +118,23 @@ class PaperOuter:
         for name in ["x", "ph", "dp", "a", "energy", "new", "t", "hs"]:
             setattr(self, name, torch.empty((n, n, n), device="cuda", dtype=torch.float64))
         self.scratch = torch.empty(4 * n ** 3 + 512, device="cuda", dtype=torch.float64)
+        self.scratch[4 * n ** 3:4 * n ** 3 + 8].zero_()  # bisection bounds and the change record
         self.steps = 0
-        self.change = 0.0
         self.raw_filter(torch.ones_like(self.x), self.hs)
+
+    @property
+    def change(self):
+        """max |new - x| of the last OC update: a (1,) device tensor, updated in place (also by
+        ``step_async``) like the reference's ``outer.change``."""
+        N = self.n ** 3
+        return self.scratch[4 * N + 4:4 * N + 5]
+
+    @property
+    def bounds(self):
+        """(lo, hi, continue flag, bisection steps) of the last OC update on the device, the layout
+        of the reference's ``outer.bounds`` (reproduction.py:77,96; outer.cu:34-38)."""
+        N = self.n ** 3
+        return self.scratch[4 * N:4 * N + 4]
 
     def raw_filter(self, x, out):
         _lib.check(_lib.lib().pgj_cone_filter(self.n, _p(self.offsets), _p(self.weights), self.weights.numel(),
@@ -137,7 +163,7 @@ class PaperOuter:
                                            self.beta, self.eta, self.emin, self.move, self.exponent, self.floor,
                                            _p(self.new), _p(self.scratch), C.byref(steps), C.byref(ch), _sp()),
                    "pgj_paper_oc")
-        self.steps, self.change = steps.value, ch.value
+        self.steps = steps.value
 
     def step_async(self, e):
         """OC update enqueued on the current stream without a host synchronisation; ``record()``
