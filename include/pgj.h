@@ -70,13 +70,35 @@ int pgj_workspace_bytes(int n, int loads, int precision, size_t* bytes);
 int pgj_ctx_create(int n, int loads, int precision, double lam, double mu,
                    void* workspace, size_t workspace_bytes, void* stream, pgj_ctx** out);
 int pgj_ctx_destroy(pgj_ctx* ctx);
+/* Batched context: `designs` independent designs of the same grid and medium, `loads` right-hand
+ * sides each, solved as designs * loads recurrences by the same kernels (every launch carries all
+ * designs). No reference counterpart: the reference batches only the loads of one design
+ * (load_mode='parallel', exp/asg_gpu_resident_20261103/resident.py:72-73) and loops over designs on
+ * the host (exp/asg_density_selector_20261105/run.py:105-119). Load l belongs to design l / loads;
+ * macros, u and info of a solve are (designs * loads) records in that order. Restarts are decided per
+ * design, and a design that took its last attempt is left untouched by the later attempts of the
+ * others, so every design's result and iteration counts are those of a solve of that design alone
+ * (same grid, precision and tile shapes). designs <= 16, loads <= 8. pgj_ctx_create is the one-design
+ * case. */
+int pgj_workspace_bytes_batch(int n, int designs, int loads, int precision, size_t* bytes);
+int pgj_ctx_create_batch(int n, int designs, int loads, int precision, double lam, double mu,
+                         void* workspace, size_t workspace_bytes, void* stream, pgj_ctx** out);
+int pgj_ctx_designs(pgj_ctx* ctx);
+/* Design d's material field (a copy of the device field a) and preconditioner exponent (its
+ * D^-alpha/2 scale); pgj_set_material / pgj_set_alpha address design 0. */
+int pgj_set_material_at(pgj_ctx* ctx, int design, const double* a, void* stream);
+int pgj_set_alpha_at(pgj_ctx* ctx, int design, double alpha, void* stream);
+/* Homogenized tensor of design d from its six Voigt solutions u (6, 3N), 36 float64 to device C. */
+int pgj_effective_tensor_at(pgj_ctx* ctx, int design, const double* u, double* C, void* stream);
+
 /* Device pointer to the context's (loads, 3N) float64 solution / warm-start block (the
  * reference's Resident.solutions, resident.py:79-82). */
 double* pgj_ctx_solutions(pgj_ctx* ctx);
-/* Device pointer to the context's (1, 3N) float64 scale field D^-alpha/2 (resident.py:88). */
+/* Device pointer to the context's (1, 3N) float64 scale field D^-alpha/2 (resident.py:88); a batched
+ * context holds one per design, (designs, 3N). */
 double* pgj_ctx_scale(pgj_ctx* ctx);
 /* Device pointer to the context's (n, n, n) float64 material field a (op._material_field,
- * solver/experiments/adaptive_green_scaling/study.py:74). */
+ * solver/experiments/adaptive_green_scaling/study.py:74); (designs, n, n, n) in a batched context. */
 double* pgj_ctx_material(pgj_ctx* ctx);
 
 /* Density multiplier a (n^3 float64, device) -> context material field; no N x 21 expansion
@@ -132,6 +154,17 @@ int pgj_set_inner_rtol(pgj_ctx* ctx, double inner_rtol);
  * (delta in (0,1), default 0.1). mode 1: restarted refinement sweeps (FP32 solve to inner_rtol,
  * u += d, FP64 residual), at most 12 sweeps. */
 int pgj_set_mixed_mode(pgj_ctx* ctx, int mode, double delta);
+/* Per-load PCG iteration cap of the context's solves (default 4000, the reference's cap,
+ * resident.py:120; 1 <= cap <= 16000). The FP64 drop-in keeps the default. No reference counterpart
+ * for other values: the mixed scheme's FP32 recurrence takes more, cheaper iterations at high
+ * contrast, and a larger cap lets it certify where the FP64 recurrence needs most of the 4000. */
+int pgj_set_iteration_cap(pgj_ctx* ctx, int cap);
+int pgj_iteration_cap(pgj_ctx* ctx);
+/* Arithmetic of the recurrence operator of a PGJ_FP32 context (no reference counterpart): 0 (default)
+ * FP32; 1 FP64 element actions and node sums on the FP32 vectors, for high-contrast designs (weak
+ * material ratios near 1e-9), where FP32 node sums of stiff and weak elements cancel. The Green
+ * apply and the vectors stay FP32. PGJ_FP64 contexts accept 1 only. */
+int pgj_set_mixed_operator(pgj_ctx* ctx, int fp64);
 /* Refinement count of the last pgj_solve: 1 for PGJ_FP64; sweeps in mixed mode 1; 1 + true-residual
  * replacements in mixed mode 0. */
 int pgj_last_refinements(pgj_ctx* ctx);
@@ -177,14 +210,14 @@ int pgj_energies(pgj_ctx* ctx, int loads, const double* u, const double* macros,
 int pgj_effective_tensor(pgj_ctx* ctx, const double* u, double* C, void* stream);
 
 /* Homogenized tensor of six Voigt solutions without any device allocation (no counterpart in the
- * reference). For callers that cannot allocate device memory: a host application that owns the
- * device memory pool and forbids third-party allocations, or code running while a CUDA graph is
- * captured, where cudaMalloc cannot be recorded. The caller passes a (n^3), u (6, 3N) and C (36
- * float64), all device; the scratch lives in a fixed file-scope device array of about 0.69 MB per
- * GPU, held until exit. Accepts 2 <= n <= 256 (PGJ_ERR_ARGUMENT otherwise). The first call on a
- * device looks up the array's device address and writes its constants (a synchronous copy), so
- * make that first call before any stream capture. All calls share the array: calls that overlap on
- * the GPU race and must be ordered on one stream. */
+ * reference). For callers that cannot allocate device memory, such as a host application that owns
+ * the device memory pool and forbids third-party allocations. The caller passes a (n^3), u (6, 3N)
+ * and C (36 float64), all device; the scratch lives in a fixed file-scope device array of about
+ * 0.69 MB per GPU, held until exit, and the unit Voigt strains in a statically initialised device
+ * table. Accepts 2 <= n <= 256 (PGJ_ERR_ARGUMENT otherwise). The first call on a device (and the
+ * first after its context is replaced, e.g. by cudaDeviceReset) looks up the array's device
+ * address, so make that first call before any stream capture. All calls share the array: calls that
+ * overlap on the GPU race and must be ordered on one stream. */
 int pgj_effective_tensor_noalloc(int n, double lam, double mu, const double* a, const double* u, double* C,
                                  void* stream);
 

@@ -113,25 +113,29 @@ def _gather(u5: np.ndarray) -> np.ndarray:
     return stacked.reshape(u5.shape[0], -1, 24)
 
 
-def _scatter(fe: np.ndarray, n: int) -> np.ndarray:
-    """(L,N,24) element forces -> (L,3N) node forces: q[node] = sum_b F[node-b, b]."""
+def _scatter(fe: np.ndarray, n: int, reverse: bool = False) -> np.ndarray:
+    """(L,N,24) element forces -> (L,3N) node forces: q[node] = sum_b F[node-b, b].
+
+    ``reverse`` sums the eight corners in the opposite order (same value, other rounding).
+    """
     L = fe.shape[0]
     f6 = fe.reshape(L, n, n, n, 8, 3)
     out = np.zeros((L, n, n, n, 3))
-    for b, (bx, by, bz) in enumerate(local_offsets()):
+    corners = list(enumerate(local_offsets()))
+    for b, (bx, by, bz) in (corners[::-1] if reverse else corners):
         out += np.roll(f6[:, :, :, :, b, :], shift=(bz, by, bx), axis=(1, 2, 3))
     return out.reshape(L, -1)
 
 
 def apply_operator(a: np.ndarray, u: np.ndarray, lam: float, mu: float,
-                   active: np.ndarray | None = None) -> np.ndarray:
+                   active: np.ndarray | None = None, reverse: bool = False) -> np.ndarray:
     """q = K(a) u for each load; inactive loads return zeros (``scalar_fi.cu:14-36``)."""
     n = a.shape[0]
     u = np.atleast_2d(u)
     ke = element_stiffness(n, lam, mu)
     ue = _gather(_as_nodes(u, n))
     fe = (ue @ ke) * a.reshape(1, -1, 1)
-    q = _scatter(fe, n)
+    q = _scatter(fe, n, reverse)
     if active is not None:
         q[~np.asarray(active, bool)] = 0.0
     return q
@@ -294,16 +298,33 @@ class Problem:
     def n(self) -> int:
         return self.a.shape[0]
 
+    reverse: bool = False
+
     def K(self, u, active=None):
-        return apply_operator(self.a, u, self.lam, self.mu, active)
+        return apply_operator(self.a, u, self.lam, self.mu, active, self.reverse)
 
     def B(self, r):
         return precondition(r, self.scale, self.symbol)
 
 
+def _dot_a(x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    return (x * y).sum(1)
+
+
+def _dot_b(x: np.ndarray, y: np.ndarray) -> np.ndarray:
+    """The same per-load dot product summed per component first, z before x (other rounding)."""
+    part = (x * y).reshape(x.shape[0], -1, 3).sum(1)
+    return part[:, 2] + part[:, 1] + part[:, 0]
+
+
 def solve_batch(prob: Problem, f: np.ndarray, u0: np.ndarray | None = None, rtol: float = 1e-8,
-                max_restarts: int = 2, iteration_cap: int = ITERATION_CAP, max_iterations: int | None = None):
+                max_restarts: int = 2, iteration_cap: int = ITERATION_CAP, max_iterations: int | None = None,
+                order: str = "a"):
     """Masked multi-load PCG with true-residual certification (``resident.py:119-136,186-209``).
+
+    ``order`` "b" runs the same recurrence with the recurrence dot products and the operator's
+    corner sums in another order: equal in exact arithmetic, rounded differently. An iteration
+    count that agrees between the two orders is stable against rounding-level perturbations.
 
     ``max_iterations`` bounds the total PCG iterations run (timing samples only); a bounded run
     returns whatever state it reached.
@@ -312,6 +333,8 @@ def solve_batch(prob: Problem, f: np.ndarray, u0: np.ndarray | None = None, rtol
     """
     L = f.shape[0]
     n = prob.n
+    dot = {"a": _dot_a, "b": _dot_b}[order]
+    prob.reverse = order == "b"
     u = np.zeros_like(f) if u0 is None else np.array(u0, dtype=np.float64)
     norm = np.sqrt((f * f).sum(1))
     target2 = np.maximum(norm * rtol, np.full_like(norm, 1e-13 / math.sqrt(n))) ** 2
@@ -327,30 +350,30 @@ def solve_batch(prob: Problem, f: np.ndarray, u0: np.ndarray | None = None, rtol
     restarts = 0
     total = 0
     while True:
-        active = ((r * r).sum(1) > target2) & (iterations < iteration_cap) & ~bad
+        active = (dot(r, r) > target2) & (iterations < iteration_cap) & ~bad
         z = prob.B(r)
         p = np.where(active[:, None], z, 0.0)
-        rz = (r * z).sum(1)
+        rz = dot(r, z)
         while active.any():
             if max_iterations is not None and total >= max_iterations:
                 break
             total += 1
             q = prob.K(p, active)
-            den = (p * q).sum(1)
+            den = dot(p, q)
             valid = np.isfinite(den) & (den > 0) & np.isfinite(rz) & (rz > 0)
             failed = active & ~valid
             with np.errstate(divide="ignore", invalid="ignore"):
                 alpha = np.where(active & valid, rz / np.where(valid, den, 1.0), 0.0)
             u = u + alpha[:, None] * p
             r = r - alpha[:, None] * q
-            res2 = (r * r).sum(1)
+            res2 = dot(r, r)
             finite = np.isfinite(res2)
             iterations = iterations + active.astype(np.int64)
             keep = active & valid & finite & (res2 > target2) & (iterations < iteration_cap)
             bad = bad | failed | (active & ~finite)
             active = keep
             z = prob.B(r)
-            newrz = (r * z).sum(1)
+            newrz = dot(r, z)
             with np.errstate(divide="ignore", invalid="ignore"):
                 beta = np.where(active, newrz / np.where(rz != 0, rz, 1.0), 0.0)
             p = np.where(active[:, None], z + beta[:, None] * p, 0.0)
@@ -407,12 +430,12 @@ def effective_tensor(a: np.ndarray, u: np.ndarray, lam: float, mu: float, macros
 
 
 def homogenize(a: np.ndarray, lam: float, mu: float, alpha: float, rtol: float = 1e-8, u0=None,
-               macros=None, max_iterations: int | None = None):
+               macros=None, max_iterations: int | None = None, order: str = "a"):
     """One certified multi-load homogenization (all loads as parallel recurrences)."""
     macros = np.eye(6) if macros is None else np.atleast_2d(macros)
     prob = Problem(a, lam, mu, alpha)
     f = rhs(prob.a, macros, lam, mu)
-    u, infos, raised = solve_batch(prob, f, u0, rtol, max_iterations=max_iterations)
+    u, infos, raised = solve_batch(prob, f, u0, rtol, max_iterations=max_iterations, order=order)
     C = effective_tensor(prob.a, u, lam, mu, macros) if macros.shape[0] == 6 else None
     return dict(u=u, infos=infos, raised=raised, C=C, f=f)
 

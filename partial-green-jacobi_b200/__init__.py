@@ -9,10 +9,10 @@ from .resident import (Backend, Operator, PaperBackend, PaperResident, Resident,
                        PAPER_MEDIUM, STUDY1_MEDIUM)
 from .outer import PaperOuter, ResidentOuter, cone_stencil, gaussian_weights
 from .designs import baseline_density, baseline_design, simp, study1_initial, study1_state0
-from .batch import Batch, Request, Result
+from .batch import Batch, BatchedOperator, Request, Result
 from . import alpha_selectors, replay_state, serve, shear_design
 
 __all__ = ["Backend", "Operator", "PaperBackend", "PaperResident", "Resident", "SelectorResident", "PaperOuter",
            "ResidentOuter", "cone_stencil", "gaussian_weights", "baseline_density", "baseline_design", "simp",
-           "study1_initial", "study1_state0", "Batch", "Request", "Result", "alpha_selectors", "replay_state",
+           "study1_initial", "study1_state0", "Batch", "BatchedOperator", "Request", "Result", "alpha_selectors", "replay_state",
            "serve", "shear_design", "ETA_ANCHORS", "PAPER_MEDIUM", "STUDY1_MEDIUM", "_lib"]

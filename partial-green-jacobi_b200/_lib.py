@@ -48,6 +48,12 @@ SIGNATURES = {
     "pgj_workspace_bytes": (C.c_int, [C.c_int, C.c_int, C.c_int, C.POINTER(sz)]),
     "pgj_ctx_create": (C.c_int, [C.c_int, C.c_int, C.c_int, f64, f64, vp, sz, vp, C.POINTER(vp)]),
     "pgj_ctx_destroy": (C.c_int, [vp]),
+    "pgj_workspace_bytes_batch": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(sz)]),
+    "pgj_ctx_create_batch": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, f64, f64, vp, sz, vp, C.POINTER(vp)]),
+    "pgj_ctx_designs": (C.c_int, [vp]),
+    "pgj_set_material_at": (C.c_int, [vp, C.c_int, vp, vp]),
+    "pgj_set_alpha_at": (C.c_int, [vp, C.c_int, f64, vp]),
+    "pgj_effective_tensor_at": (C.c_int, [vp, C.c_int, vp, vp, vp]),
     "pgj_ctx_solutions": (vp, [vp]),
     "pgj_ctx_scale": (vp, [vp]),
     "pgj_ctx_material": (vp, [vp]),
@@ -63,6 +69,9 @@ SIGNATURES = {
     "pgj_solve_wait": (C.c_int, [vp, C.POINTER(LoadInfo), vp]),
     "pgj_set_inner_rtol": (C.c_int, [vp, f64]),
     "pgj_set_mixed_mode": (C.c_int, [vp, C.c_int, f64]),
+    "pgj_set_mixed_operator": (C.c_int, [vp, C.c_int]),
+    "pgj_set_iteration_cap": (C.c_int, [vp, C.c_int]),
+    "pgj_iteration_cap": (C.c_int, [vp]),
     "pgj_last_refinements": (C.c_int, [vp]),
     "pgj_last_launches": (C.c_longlong, [vp]),
     "pgj_selftest_wait_timeout": (C.c_int, [vp, C.c_int, vp]),

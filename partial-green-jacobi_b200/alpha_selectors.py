@@ -2,8 +2,11 @@
 pick the one exponent alpha of the partial Green-Jacobi scaling D^{-alpha/2} for a design.
 
 They follow ``exp/asg_density_selector_20261105/run.py:27-43,53-67`` (contrast, gray, compact8 and
-compact8q; the frozen parameters of ``MODELS_FROZEN.json``) and the compact-law features of
-``solver/experiments/global_alpha_compact_law/law.py:10-19``. Each returns a 0-d float64 tensor on
+compact8q; the frozen parameters of ``MODELS_FROZEN.json``), the compact-law features of
+``solver/experiments/global_alpha_compact_law/law.py:10-19`` and the ASG MLP
+(``exp/asg_gpu_resident_20261103/resident.py:160-162``: the 92 full-grid statistics of
+``solver/experiments/global_alpha_stats/features.py:17-49`` through the frozen network of
+``solver/experiments/asg_independent/train.py:27-35``, weights in ``asg_weights``). Each returns a 0-d float64 tensor on
 the input's device. They are device-agnostic torch reductions over N values (one scalar per design
 step, off the PCG path), run on the design's own device without a host round trip.
 """
@@ -94,6 +97,84 @@ def compact8_alpha(a, quantize=False):
     if quantize:
         value = (16 * value + 0.5).floor() / 16
     return value
+
+
+# ASG features: CDF points of q, shifts of the periodic differences (in cells: 1, 2, n/16, n/8)
+ASG_CDF = (0.01, 0.05, 0.25, 0.5, 0.75, 0.95, 0.99)
+
+
+def asg_features(a):
+    """The 92 statistics of the log density rescaled to q in [0, 1], in FP32 like the reference:
+    mean and variance of q, 7 CDF values; per axis (z, y, x) and shift (1, 2, n/16, n/8 cells) of the
+    periodic difference d: mean |d|, mean d^2, mean d^4, max |d|, fraction |d| > 1e-6, fraction
+    |d| > 0.25; per axis the scaling exponent log2(s2(2) / s2(1)) and the jump ratio s2 / s1 at
+    shift 1; the three normalised cross-correlations of the unit-shift differences; the log contrast
+    over log 1e4 and 1 / n. Needs n >= 32 and n a multiple of 16 (the reference asserts the same)."""
+    torch = _torch()
+    ell = a.float().log()
+    lo, hi = torch.aminmax(ell)
+    span = hi - lo
+    q = (ell - lo) / span.clamp_min(1e-12)
+    n = q.shape[0]
+    if q.shape != (n, n, n) or n < 32 or n % 16:
+        raise ValueError("the ASG features need a cubic grid with n >= 32 and n a multiple of 16")
+    mean = q.mean()
+    values = [mean, (q - mean).square().mean()]
+    values += [(q <= t).float().mean() for t in ASG_CDF]
+    pairs, unit = [], []
+    for axis in range(3):
+        sums = []
+        for shift in (1, 2, max(1, n // 16), max(1, n // 8)):
+            diff = torch.roll(q, -shift, axis) - q
+            d = diff.abs()
+            s1, s2 = d.mean(), d.square().mean()
+            values += [s1, s2, d.square().square().mean(), d.amax(), (d > 1e-6).float().mean(),
+                       (d > 0.25).float().mean()]
+            sums.append((s1, s2))
+            if shift == 1:
+                unit.append(diff)
+        s1, s2 = sums[0]
+        exponent = torch.where(s2 > 1e-20, (sums[1][1] / s2.clamp_min(1e-20)).clamp_min(1e-20).log2(),
+                               torch.zeros_like(s2))
+        pairs += [exponent, s2 / s1.clamp_min(1e-20)]
+    values += pairs
+    norm = (unit[0].square().mean() + unit[1].square().mean() + unit[2].square().mean()).clamp_min(1e-20)
+    values += [(unit[0] * unit[1]).mean() / norm, (unit[0] * unit[2]).mean() / norm,
+               (unit[1] * unit[2]).mean() / norm, span / math.log(10000.0), q.new_tensor(1.0 / n)]
+    return torch.stack(values)
+
+
+_ASG_NET = {}
+
+
+def _asg_net(device):
+    """The frozen MLP's tensors on `device` (loaded and checked once per device)."""
+    torch = _torch()
+    key = str(device)
+    if key not in _ASG_NET:
+        from . import asg_weights
+
+        w = asg_weights.load()
+        _ASG_NET[key] = {k: (torch.tensor(v, device=device) if k != "threshold" else v) for k, v in w.items()}
+    return _ASG_NET[key]
+
+
+def asg_prediction(a):
+    """Raw MLP output in (0, 1): sigmoid(L2 silu(L1 silu(L0 ((x - mean) / std * mask)))), FP32."""
+    torch = _torch()
+    net = _asg_net(a.device)
+    x = (asg_features(a) - net["mean"]) / net["std"] * net["mask"]
+    h = torch.nn.functional.silu(net["w0"] @ x + net["b0"])
+    h = torch.nn.functional.silu(net["w1"] @ h + net["b1"])
+    return torch.sigmoid(net["w2"] @ h + net["b2"]).reshape(())
+
+
+def asg_alpha(a):
+    """ASG alpha: the MLP prediction, or 0 (the plain Green preconditioner) below the frozen
+    threshold 0.2 (resident.py:160-162); a 0-d float64 tensor on the input's device."""
+    torch = _torch()
+    pred = asg_prediction(a)
+    return torch.where(pred < _asg_net(a.device)["threshold"], torch.zeros_like(pred), pred).double()
 
 
 def _torch():

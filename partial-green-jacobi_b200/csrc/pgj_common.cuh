@@ -12,7 +12,9 @@
 
 namespace pgj {
 
-constexpr int kMaxLoads = 8;
+constexpr int kMaxLoads = 8;          // right-hand sides per design
+constexpr int kMaxDesigns = 16;       // designs of one batched context
+constexpr int kMaxTotalLoads = kMaxLoads * kMaxDesigns;
 constexpr int kMaxStages = 8;
 
 __host__ __device__ __forceinline__ int wrapi(int x, int n) { return x < 0 ? x + n : (x >= n ? x - n : x); }
@@ -164,6 +166,8 @@ struct LoadScalars {
   int reliable;     // mixed: replace the FP32 recurrence residual by the FP64 true residual now
   double anchor;    // mixed: recurrence ||r||^2 at the last true-residual replacement
   int total_iterations;  // mixed refinement: inner iterations summed over sweeps
+  int frozen;       // batched contexts: this load's design took its last attempt (later attempts skip it)
+  int restarts;     // restarts taken by this load's design
   int ticket[8];    // per-kernel block tickets for the last-block finalizers
 };
 

@@ -43,7 +43,26 @@ struct Graphs {
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-static Layout make_layout(int n, int L, int prec) {
+DesignScope::DesignScope(pgj_ctx* ctx, int d) : c(ctx), a(ctx->a), scale(ctx->scale), scale32(ctx->scale32), shat(ctx->shat) {
+  const size_t N = size_t(c->N), nsp = size_t(c->ns + (c->ns & 1));
+  const size_t tsz = c->prec == PGJ_FP32 ? 4 : 8;
+  c->a = a + d * N;
+  c->scale = scale + d * 3 * N;
+  if (scale32) c->scale32 = scale32 + d * 3 * N;
+  c->shat = static_cast<char*>(shat) + d * 2 * tsz * 3 * size_t(c->n) * c->n * nsp;
+}
+
+DesignScope::~DesignScope() {
+  c->a = a;
+  c->scale = scale;
+  c->scale32 = scale32;
+  c->shat = shat;
+}
+
+// D designs of `lpd` loads each: per-design fields (a, scale, scale32, shat) are D blocks, per-load
+// fields L = D lpd blocks.
+static Layout make_layout(int n, int D, int lpd, int prec) {
+  const int L = D * lpd;
   Layout y;
   const size_t N = size_t(n) * n * n, N3 = 3 * N;
   const size_t ns = size_t(n / 2 + 1), Nh = size_t(n) * n * ns;
@@ -59,8 +78,8 @@ static Layout make_layout(int n, int L, int prec) {
   y.tw = take(size_t(n) * (sizeof(double2) + sizeof(float2) + sizeof(float4)));
   const size_t pslots = size_t(4 * L > 24 ? 4 * L : 24);
   y.partials = take(sizeof(double) * pslots * kMaxPartials);
-  y.a = take(sizeof(double) * N);
-  y.scale = take(sizeof(double) * N3);
+  y.a = take(sizeof(double) * N * D);
+  y.scale = take(sizeof(double) * N3 * D);
   y.symbol = take(sizeof(double) * 6 * Nh);
   y.symbol32 = take(prec == PGJ_FP32 ? sizeof(float) * 6 * Nh : 0);
   y.solutions = take(sizeof(double) * N3 * L);
@@ -73,8 +92,8 @@ static Layout make_layout(int n, int L, int prec) {
   y.q = take(tsz * N3 * L);
   y.sw = take(tsz * N3 * L);
   y.spec = take(2 * tsz * 3 * size_t(n) * n * nsp * L);
-  y.shat = take(2 * tsz * 3 * size_t(n) * n * nsp);
-  y.scale32 = take(prec == PGJ_FP32 ? sizeof(float) * N3 : 0);
+  y.shat = take(2 * tsz * 3 * size_t(n) * n * nsp * D);
+  y.scale32 = take(prec == PGJ_FP32 ? sizeof(float) * N3 * D : 0);
   y.total = o;
   return y;
 }
@@ -113,14 +132,18 @@ static int capture_iteration(pgj_ctx* c, int L, cudaStream_t s, cudaGraphConditi
 // First direction p = M r of a recurrence (the masks are set): unfused Green + p = z, or the fused
 // form, which first refreshes DFT(s) in case the scale field was rewritten through its view.
 static long long first_direction_launches(const pgj_ctx* c) {
-  return c->fused ? (c->prec == PGJ_FP32 ? 7 : 6) : 6;  // DFT(s) (3) [+ FP32 scale] + 3, or Green (5) + p
+  // per design DFT(s) (3) [+ FP32 scale], then 3; or Green (5) + p
+  return c->fused ? (long long)c->D * (c->prec == PGJ_FP32 ? 4 : 3) + 3 : 6;
 }
 
 static int capture_first_direction(pgj_ctx* c, int L, cudaStream_t s) {
   int st;
   if (c->fused) {
-    if ((st = build_shat(c, s))) return st;
-    if (c->prec == PGJ_FP32 && (st = launch_scale32(c, s))) return st;
+    for (int d = 0; d < c->D; ++d) {
+      DesignScope view(c, d);
+      if ((st = build_shat(c, s))) return st;
+      if (c->prec == PGJ_FP32 && (st = launch_scale32(c, s))) return st;
+    }
     if ((st = launch_fxy(c, L, c->prec, kSlabInitL, nullptr, s))) return st;
     if ((st = launch_fz_fused(c, L, c->prec, true, s))) return st;
     return launch_ifxy(c, L, c->prec, true, s, 0, false);
@@ -380,26 +403,32 @@ static bool grid_ok(int n) {
   return n >= 4 && n <= 256 && make_fft_plan(n, &p);
 }
 
-int pgj_workspace_bytes(int n, int loads, int precision, size_t* bytes) {
-  if (!bytes || loads < 1 || loads > kMaxLoads || (precision != PGJ_FP64 && precision != PGJ_FP32))
-    return PGJ_ERR_ARGUMENT;
+static bool batch_ok(int designs, int loads, int precision) {
+  return designs >= 1 && designs <= kMaxDesigns && loads >= 1 && loads <= kMaxLoads &&
+         (precision == PGJ_FP64 || precision == PGJ_FP32);
+}
+
+int pgj_workspace_bytes_batch(int n, int designs, int loads, int precision, size_t* bytes) {
+  if (!bytes || !batch_ok(designs, loads, precision)) return PGJ_ERR_ARGUMENT;
   if (!grid_ok(n)) return PGJ_ERR_UNSUPPORTED;
-  *bytes = make_layout(n, loads, precision).total;
+  *bytes = make_layout(n, designs, loads, precision).total;
   return PGJ_OK;
 }
 
-int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void* workspace, size_t workspace_bytes,
-                   void* stream, pgj_ctx** out) {
-  if (!out || loads < 1 || loads > kMaxLoads || !(mu > 0) || !(lam + 2 * mu / 3 > 0) ||
-      (precision != PGJ_FP64 && precision != PGJ_FP32))
-    return PGJ_ERR_ARGUMENT;
+int pgj_workspace_bytes(int n, int loads, int precision, size_t* bytes) {
+  return pgj_workspace_bytes_batch(n, 1, loads, precision, bytes);
+}
+
+int pgj_ctx_create_batch(int n, int designs, int loads, int precision, double lam, double mu, void* workspace,
+                         size_t workspace_bytes, void* stream, pgj_ctx** out) {
+  if (!out || !batch_ok(designs, loads, precision) || !(mu > 0) || !(lam + 2 * mu / 3 > 0)) return PGJ_ERR_ARGUMENT;
   if (!grid_ok(n)) return PGJ_ERR_UNSUPPORTED;
-  Layout y = make_layout(n, loads, precision);
+  Layout y = make_layout(n, designs, loads, precision);
   if (!workspace || workspace_bytes < y.total || (reinterpret_cast<uintptr_t>(workspace) & 255)) return PGJ_ERR_WORKSPACE;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   pgj_ctx* c = new (std::nothrow) pgj_ctx();
   if (!c) return PGJ_ERR_ARGUMENT;
-  c->n = n; c->L = loads; c->prec = precision; c->lam = lam; c->mu = mu;
+  c->n = n; c->D = designs; c->lpd = loads; c->L = designs * loads; c->prec = precision; c->lam = lam; c->mu = mu;
   c->N = (long long)n * n * n; c->ns = n / 2 + 1; c->Nh = (long long)n * n * c->ns;
   c->kc = make_opconst(n, lam, mu);
   make_fft_plan(n, &c->plan);
@@ -423,16 +452,18 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
   c->scale32 = precision == PGJ_FP32 ? reinterpret_cast<float*>(b + y.scale32) : nullptr;
   c->partials = reinterpret_cast<double*>(b + y.partials);
   c->scal_out = reinterpret_cast<LoadScalars*>(b + y.scal);
-  c->scal_in = c->scal_out + loads;
+  c->scal_in = c->scal_out + c->L;
   c->scal = c->scal_out;
   c->d = precision == PGJ_FP32 ? static_cast<void*>(b + y.d) : nullptr;
   c->macros = reinterpret_cast<double*>(b + y.macros);
   c->cond = reinterpret_cast<int*>(b + y.cond);
   c->aux = reinterpret_cast<double*>(b + y.aux);
   c->alpha = 0.0;
+  for (int d = 0; d < kMaxDesigns; ++d) c->alphas[d] = 0.0;
   c->inner_rtol = 1e-5;
   c->rel_delta2 = precision == PGJ_FP32 ? 1e-2 : 0.0;
   c->mixed_mode = 0;
+  c->cap = 4000;  // the reference's per-load iteration cap (resident.py)
   c->last_refinements = 0;
   c->graphs = new (std::nothrow) Graphs();
   int st = PGJ_OK;
@@ -454,7 +485,10 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
     if (e != cudaSuccess) st = set_cuda_error(e);
   }
   if (!st) st = launch_scale(c, 0.5, s);  // stages the diagonal constants (once)
-  if (!st) st = launch_scale(c, 0.0, s);  // scale = 1 until an alpha is selected
+  for (int d = 0; d < designs && !st; ++d) {
+    DesignScope view(c, d);
+    st = launch_scale(c, 0.0, s);  // scale = 1 until an alpha is selected
+  }
   if (!st) st = autotune_stencil(c, s);
   if (!st) st = autotune_fft(c, s);
   if (st) {
@@ -465,6 +499,13 @@ int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void*
   *out = c;
   return PGJ_OK;
 }
+
+int pgj_ctx_create(int n, int loads, int precision, double lam, double mu, void* workspace, size_t workspace_bytes,
+                   void* stream, pgj_ctx** out) {
+  return pgj_ctx_create_batch(n, 1, loads, precision, lam, mu, workspace, workspace_bytes, stream, out);
+}
+
+int pgj_ctx_designs(pgj_ctx* ctx) { return ctx ? ctx->D : -1; }
 
 int pgj_ctx_destroy(pgj_ctx* ctx) {
   if (!ctx) return PGJ_ERR_ARGUMENT;
@@ -477,18 +518,24 @@ double* pgj_ctx_solutions(pgj_ctx* ctx) { return ctx ? ctx->solutions : nullptr;
 double* pgj_ctx_scale(pgj_ctx* ctx) { return ctx ? ctx->scale : nullptr; }
 double* pgj_ctx_material(pgj_ctx* ctx) { return ctx ? ctx->a : nullptr; }
 
-int pgj_set_material(pgj_ctx* c, const double* a, void* stream) {
-  if (!c || !a) return PGJ_ERR_ARGUMENT;
-  cudaError_t e = cudaMemcpyAsync(c->a, a, sizeof(double) * size_t(c->N), cudaMemcpyDeviceToDevice,
-                                  static_cast<cudaStream_t>(stream));
+int pgj_set_material_at(pgj_ctx* c, int design, const double* a, void* stream) {
+  if (!c || !a || design < 0 || design >= c->D) return PGJ_ERR_ARGUMENT;
+  cudaError_t e = cudaMemcpyAsync(c->a + size_t(design) * size_t(c->N), a, sizeof(double) * size_t(c->N),
+                                  cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream));
   return e == cudaSuccess ? PGJ_OK : set_cuda_error(e);
 }
 
-int pgj_set_alpha(pgj_ctx* c, double alpha, void* stream) {
-  if (!c || !std::isfinite(alpha)) return PGJ_ERR_ARGUMENT;
-  c->alpha = alpha;
+int pgj_set_material(pgj_ctx* c, const double* a, void* stream) { return pgj_set_material_at(c, 0, a, stream); }
+
+int pgj_set_alpha_at(pgj_ctx* c, int design, double alpha, void* stream) {
+  if (!c || !std::isfinite(alpha) || design < 0 || design >= c->D) return PGJ_ERR_ARGUMENT;
+  c->alphas[design] = alpha;
+  if (design == 0) c->alpha = alpha;
+  DesignScope view(c, design);
   return launch_scale(c, alpha, static_cast<cudaStream_t>(stream));
 }
+
+int pgj_set_alpha(pgj_ctx* c, double alpha, void* stream) { return pgj_set_alpha_at(c, 0, alpha, stream); }
 
 int pgj_apply(pgj_ctx* c, int loads, const double* p, const int32_t* active, double* q, void* stream) {
   if (!c || !p || !q || loads < 1 || loads > c->L) return PGJ_ERR_ARGUMENT;
@@ -541,6 +588,25 @@ int pgj_set_inner_rtol(pgj_ctx* c, double inner_rtol) {
 
 int pgj_last_refinements(pgj_ctx* c) { return c ? c->last_refinements : -1; }
 
+int pgj_set_iteration_cap(pgj_ctx* c, int cap) {
+  if (!c || cap < 1 || cap > 16000) return PGJ_ERR_ARGUMENT;
+  c->cap = cap;
+  c->graphs->loads = 0;  // the cap is a parameter of the captured kernels
+  c->graphs->attempt_loads = 0;
+  return PGJ_OK;
+}
+
+int pgj_iteration_cap(pgj_ctx* c) { return c ? c->cap : -1; }
+
+int pgj_set_mixed_operator(pgj_ctx* c, int fp64) {
+  if (!c || (fp64 != 0 && fp64 != 1)) return PGJ_ERR_ARGUMENT;
+  if (c->prec != PGJ_FP32) return fp64 ? PGJ_OK : PGJ_ERR_UNSUPPORTED;  // FP64 contexts are FP64 throughout
+  c->op64 = fp64;
+  c->graphs->loads = 0;  // rebuild the solve graphs with the other operator
+  c->graphs->attempt_loads = 0;
+  return PGJ_OK;
+}
+
 int pgj_set_mixed_mode(pgj_ctx* c, int mode, double delta) {
   if (!c || (mode != 0 && mode != 1) || !(delta > 0 && delta < 1)) return PGJ_ERR_ARGUMENT;
   c->mixed_mode = mode;
@@ -556,6 +622,7 @@ static constexpr int kMaxSweeps = 12;
 
 int pgj_solve_async(pgj_ctx* c, int loads, const double* macros, double rtol, double* u, void* stream) {
   if (!c || !macros || !u || loads < 1 || loads > c->L || !(rtol > 0)) return PGJ_ERR_ARGUMENT;
+  if (c->D > 1 && loads % c->lpd != 0) return PGJ_ERR_ARGUMENT;  // whole designs of a batched context
   if (c->prec == PGJ_FP32 && c->mixed_mode == 1) return PGJ_ERR_UNSUPPORTED;  // sweeps need the host
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   const size_t bytes = sizeof(double) * 3 * size_t(c->N) * loads;
@@ -593,7 +660,7 @@ int pgj_solve_wait(pgj_ctx* c, pgj_load_info* info, void* stream) {
     I.relative_residual = h[l].absolute / (h[l].norm > 1e-300 ? h[l].norm : 1e-300);
     I.iterations = h[l].iterations;
     I.converged = ok;
-    I.restarts = cnt[4];
+    I.restarts = h[l].restarts;
     I.bad = h[l].bad;
     all = all && ok;
   }
@@ -615,6 +682,7 @@ int pgj_solve_wait(pgj_ctx* c, pgj_load_info* info, void* stream) {
 
 int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* u, pgj_load_info* info, void* stream) {
   if (!c || !macros || !u || !info || loads < 1 || loads > c->L || !(rtol > 0)) return PGJ_ERR_ARGUMENT;
+  if (c->D > 1 && c->prec == PGJ_FP32 && c->mixed_mode == 1) return PGJ_ERR_UNSUPPORTED;
   if (!(c->prec == PGJ_FP32 && c->mixed_mode == 1)) {
     const int st = pgj_solve_async(c, loads, macros, rtol, u, stream);
     return st ? st : pgj_solve_wait(c, info, stream);
@@ -653,7 +721,7 @@ int pgj_solve(pgj_ctx* c, int loads, const double* macros, double rtol, double* 
       all = all && ok[l];
       anybad = anybad || h[l].bad;
       const int its = mixed ? h[l].total_iterations : h[l].iterations;
-      capped = capped || (!ok[l] && its >= 4000);
+      capped = capped || (!ok[l] && its >= c->cap);
     }
   };
   if (mixed) {
@@ -829,9 +897,14 @@ int pgj_energies(pgj_ctx* c, int loads, const double* u, const double* macros, d
   return launch_energies(c, loads, u, c->macros, e, s);
 }
 
+int pgj_effective_tensor_at(pgj_ctx* c, int design, const double* u, double* C, void* stream) {
+  if (!c || !u || !C || design < 0 || design >= c->D) return PGJ_ERR_ARGUMENT;
+  return launch_effective_tensor(c, c->a + size_t(design) * size_t(c->N), u, C, nullptr,
+                                 static_cast<cudaStream_t>(stream));
+}
+
 int pgj_effective_tensor(pgj_ctx* c, const double* u, double* C, void* stream) {
-  if (!c || !u || !C) return PGJ_ERR_ARGUMENT;
-  return launch_effective_tensor(c, u, C, nullptr, static_cast<cudaStream_t>(stream));
+  return pgj_effective_tensor_at(c, 0, u, C, stream);
 }
 
 }  // extern "C"

@@ -148,8 +148,9 @@ int launch_energies(pgj_ctx* c, int loads, const double* u, const double* macros
   return check_launch();
 }
 
-int launch_effective_tensor(pgj_ctx* c, const double* u, double* C, double* e, cudaStream_t s) {
+int launch_effective_tensor(pgj_ctx* c, const double* a, const double* u, double* C, double* e, cudaStream_t s) {
   EnergyArgs A = energy_args(c, 6, u, c->aux + kAuxVoigt);  // unit Voigt macros (6 x 6)
+  A.a = a;
   A.C = C;
   A.e = e;
   unsigned blocks = 4 * 148;
@@ -169,12 +170,11 @@ int launch_effective_tensor(pgj_ctx* c, const double* u, double* C, double* e, c
 //
 // Some callers cannot allocate device memory: a host application that owns the whole device
 // memory pool and forbids third-party cudaMalloc (for instance a finite-element code that calls
-// this library as a post-processing plugin inside its own memory budget), or code that has to
-// run while a CUDA graph is being captured, where cudaMalloc is not a capturable operation. They
-// still hold the density field and the six solutions, and want C_H from them. This entry point
-// runs the same C_H kernel as pgj_effective_tensor, with its scratch (block partial sums, the
-// last-block ticket and the six unit Voigt strains) in a fixed file-scope device array instead of
-// a context workspace.
+// this library as a post-processing plugin inside its own memory budget). They still hold the
+// density field and the six solutions, and want C_H from them. This entry point runs the same C_H
+// kernel as pgj_effective_tensor, with its scratch (block partial sums and the last-block ticket)
+// in a fixed file-scope device array instead of a context workspace; the six unit Voigt strains
+// are a statically initialised device table, so nothing has to be copied before the first call.
 //
 // Limits and sharing: the array is kNoAllocScratchBytes (about 0.69 MB) on every GPU that loads
 // the library, held until the process exits; it fits the kernel's partial sums for any grid the
@@ -182,38 +182,76 @@ int launch_effective_tensor(pgj_ctx* c, const double* u, double* C, double* e, c
 // keeps the last call's contents; the ticket is cleared at the start of each call. Two calls whose
 // work overlaps on the GPU (for example on two streams without ordering) race on the array and
 // give wrong results: order them on one stream or synchronise between them.
+#include <mutex>
+
 namespace {
 constexpr size_t kNoAllocPartialDoubles = size_t(21) * pgj::kMaxPartials;
-constexpr size_t kNoAllocVoigtDoubles = 64;
 constexpr size_t kNoAllocScalarBytes = 256;
-constexpr size_t kNoAllocScratchBytes =
-    kNoAllocPartialDoubles * sizeof(double) + kNoAllocVoigtDoubles * sizeof(double) + kNoAllocScalarBytes;
+constexpr size_t kNoAllocScratchBytes = kNoAllocPartialDoubles * sizeof(double) + kNoAllocScalarBytes;
 static_assert(sizeof(pgj::LoadScalars) <= kNoAllocScalarBytes, "scalar record must fit its slot");
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+// (6, 6) unit engineering Voigt strains, one row per load
+static __device__ const double g_noalloc_voigt[36] = {1, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0,
+                                                      0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 1};
 
+// Device addresses of the two symbols, looked up once per device with that device current and
+// kept together with the id of the context they belong to: a replaced context (cudaDeviceReset,
+// a new primary context) has another id, and the lookup is redone. The host-side names of the
+// symbols are stand-ins, never passed to a kernel. A mutex orders first calls from several threads.
 constexpr int kNoAllocMaxDevices = 64;
-// Device address of g_noalloc_scratch per device ordinal, obtained once with that device current.
-// The host-side name g_noalloc_scratch is only a stand-in for the symbol and is never passed to
-// a kernel.
-unsigned char* g_noalloc_addr[kNoAllocMaxDevices] = {nullptr};
+struct NoAllocSlot {
+  unsigned long long ctx_id = 0;
+  unsigned char* scratch = nullptr;
+  const double* voigt = nullptr;
+};
+NoAllocSlot g_noalloc_slot[kNoAllocMaxDevices];
+std::mutex g_noalloc_mutex;
 
-int noalloc_setup(int device, unsigned char** out) {
-  if (g_noalloc_addr[device]) {
-    *out = g_noalloc_addr[device];
+// Current context id through the driver entry points the runtime exposes (no libcuda link).
+// Returns 0 when the thread has no current context yet.
+unsigned long long current_context_id() {
+  using GetCurrent = int (*)(void**);
+  using GetId = int (*)(void*, unsigned long long*);
+  static GetCurrent get_current = nullptr;
+  static GetId get_id = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_current = reinterpret_cast<GetCurrent>(f);
+    if (cudaGetDriverEntryPoint("cuCtxGetId", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      get_id = reinterpret_cast<GetId>(f);
+  });
+  void* ctx = nullptr;
+  unsigned long long id = 0;
+  if (!get_current || !get_id || get_current(&ctx) != 0 || !ctx || get_id(ctx, &id) != 0) return 0;
+  return id;
+}
+
+int noalloc_setup(int device, unsigned char** scratch, const double** voigt) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  NoAllocSlot& slot = g_noalloc_slot[device];
+  unsigned long long id = current_context_id();
+  if (id != 0 && slot.ctx_id == id && slot.scratch) {
+    *scratch = slot.scratch;
+    *voigt = slot.voigt;
     return PGJ_OK;
   }
   void* p = nullptr;
+  void* v = nullptr;
   cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e == cudaSuccess) e = cudaGetSymbolAddress(&v, g_noalloc_voigt);
   if (e != cudaSuccess) return pgj::set_cuda_error(e);
-  unsigned char* base = static_cast<unsigned char*>(p);
-  double eye[36] = {0};
-  for (int i = 0; i < 6; ++i) eye[i * 6 + i] = 1.0;
-  // synchronous copy: done once per device, before any stream capture by contract
-  e = cudaMemcpy(base + kNoAllocPartialDoubles * sizeof(double), eye, sizeof(eye), cudaMemcpyHostToDevice);
-  if (e != cudaSuccess) return pgj::set_cuda_error(e);
-  g_noalloc_addr[device] = base;
-  *out = base;
+  if (id == 0) id = current_context_id();  // the lookup made the device's context current
+  slot.ctx_id = id;
+  slot.scratch = static_cast<unsigned char*>(p);
+  slot.voigt = static_cast<const double*>(v);
+  *scratch = slot.scratch;
+  *voigt = slot.voigt;
   return PGJ_OK;
 }
 }  // namespace
@@ -227,12 +265,12 @@ extern "C" int pgj_effective_tensor_noalloc(int n, double lam, double mu, const 
   if (e != cudaSuccess) return pgj::set_cuda_error(e);
   if (device < 0 || device >= kNoAllocMaxDevices) return PGJ_ERR_UNSUPPORTED;
   unsigned char* base = nullptr;
-  int st = noalloc_setup(device, &base);
+  const double* voigt = nullptr;
+  int st = noalloc_setup(device, &base, &voigt);
   if (st) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double* partials = reinterpret_cast<double*>(base);
-  double* voigt = partials + kNoAllocPartialDoubles;
-  pgj::LoadScalars* scal = reinterpret_cast<pgj::LoadScalars*>(voigt + kNoAllocVoigtDoubles);
+  pgj::LoadScalars* scal = reinterpret_cast<pgj::LoadScalars*>(partials + kNoAllocPartialDoubles);
   // the last-block ticket must start at zero
   e = cudaMemsetAsync(scal, 0, sizeof(pgj::LoadScalars), s);
   if (e != cudaSuccess) return pgj::set_cuda_error(e);

@@ -94,10 +94,11 @@ FFTGeom fft_geom(int n, int elem_bytes, const FFTPlan& plan, int rb_req, int nky
 
 struct GreenArgs {
   int n, ns, nsp;  // grid edge, half-spectrum length, padded (even) spectrum row length
+  int lpd;         // loads per design: load l uses the scale field (and DFT(s)) of design l / lpd
   FFTPlan plan;
   FFTGeom geo;
   const void* r;         // (L,3N) T input residual
-  const double* scale;   // (3N) fp64 scale field
+  const double* scale;   // (designs, 3N) fp64 scale field
   void* spec;            // (L,3,n,n,ns) complex T
   const void* sym;       // (6,Nh) T symbol
   const void* tw;        // n complex T twiddles (forward)
@@ -110,7 +111,7 @@ struct GreenArgs {
   int finalize_fz;       // FZ last block forms rz / beta (recurrence use only)
   // slab-fused recurrence (the x/y transforms run in the PCG update kernels): the spectrum holds
   // DFT(s.r); FZ subtracts mean_r . shat (shat = DFT(s)) and forms mean(s.w) by Parseval
-  const void* shat;      // (3, n, n, nsp) complex T: DFT of each component of the scale field
+  const void* shat;      // (designs, 3, n, n, nsp) complex T: DFT of each component of the scale field
   int fused;
   int forward_only;      // FZ: forward transform along z only (builds shat)
   int unit_input;        // FX: transform s itself (r ignored; builds shat)
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(512) k_fx(const GreenArgs A) {
   const size_t N = size_t(n) * n * n;
   const size_t row0 = size_t(blockIdx.x) * rb;
   const T* r = reinterpret_cast<const T*>(A.r) + size_t(load) * 3 * N;
-  const double* sc = A.scale;
+  const double* sc = A.scale + size_t(load / A.lpd) * 3 * N;
   T m[3] = {T(0), T(0), T(0)};
   if (A.use_mean) { m[0] = T(A.scal[load].mean_r[0]); m[1] = T(A.scal[load].mean_r[1]); m[2] = T(A.scal[load].mean_r[2]); }
   const int total = rb * 3 * n;
@@ -241,7 +242,7 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
   }
   // symbol multiply and Parseval partial sums: rows kz over (threadIdx.y, threadIdx.z)
   const T* sym = reinterpret_cast<const T*>(A.sym);
-  const C* sh = reinterpret_cast<const C*>(A.shat);
+  const C* sh = reinterpret_cast<const C*>(A.shat) + size_t(load / A.lpd) * 3 * plane;
   const size_t Nh = size_t(n) * n * ns;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   if (kl < kn) {
@@ -403,7 +404,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_fz64(const GreenArgs A) {
   }
   // symbol multiply and the Parseval sums on the lane's own column
   const T* sym = reinterpret_cast<const T*>(A.sym);
-  const C* sh = reinterpret_cast<const C*>(A.shat);
+  const C* sh = reinterpret_cast<const C*>(A.shat) + size_t(load / A.lpd) * 3 * plane;
   const size_t Nh = size_t(N) * N * ns;
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
   if (valid) {
@@ -548,7 +549,7 @@ __global__ void __launch_bounds__(512) k_ifx(const GreenArgs A) {
   const C* tw = reinterpret_cast<const C*>(A.tw);
   C* res = fft_line<T>(b0, b1, threadIdx.x * pitch, 1, A.plan, tw, true);
   T* sw = reinterpret_cast<T*>(A.sw) + size_t(load) * 3 * N;
-  const double* sc = A.scale;
+  const double* sc = A.scale + size_t(load / A.lpd) * 3 * N;
   double acc[3] = {0.0, 0.0, 0.0};
   const int tot2 = rb * 3 * n;
   const size_t gbase = row0 * n * 3;
@@ -654,6 +655,7 @@ static GreenArgs green_args(pgj_ctx* c, int prec, const void* r) {
   GreenArgs A;
   std::memset(&A, 0, sizeof(A));
   A.n = c->n; A.ns = c->ns; A.nsp = c->ns + (c->ns & 1); A.plan = c->plan; A.geo = c->fg;
+  A.lpd = c->lpd;
   A.r = r; A.scale = c->scale; A.spec = c->spec;
   A.sym = prec == PGJ_FP32 ? static_cast<const void*>(c->symbol32) : static_cast<const void*>(c->symbol);
   A.tw = prec == PGJ_FP32 ? static_cast<const void*>(static_cast<double2*>(c->tw) + c->n) : c->tw;
@@ -735,13 +737,14 @@ int launch_green_standalone(pgj_ctx* c, int loads, const double* r, double* z, c
   return check_launch();
 }
 
-// Green-apply autotuner: times the five passes (all loads active) for candidate tile shapes
-// (rows per x block, y-chunks, z-chunks) on the context's buffers; cached per (n, loads, precision).
+// Green-apply autotuner: times the five passes (the loads of one design, all active) for candidate
+// tile shapes (rows per x block, y-chunks, z-chunks) on the context's buffers; cached per (n, loads
+// per design, precision), so batched contexts share the choice with single ones.
 static std::mutex g_fft_mutex;
 static std::map<std::tuple<int, int, int>, FFTGeom> g_fft_tuned;
 
 int autotune_fft(pgj_ctx* c, cudaStream_t s) {
-  const auto key = std::make_tuple(c->n, c->L, c->prec);
+  const auto key = std::make_tuple(c->n, c->lpd, c->prec);
   {
     std::lock_guard<std::mutex> lock(g_fft_mutex);
     auto it = g_fft_tuned.find(key);
@@ -769,17 +772,17 @@ int autotune_fft(pgj_ctx* c, cudaStream_t s) {
   FFTGeom best = c->fg;
   float best_ms = 1e30f;
   for (int r = 0; r < 10; ++r)  // bring the clocks up before timing anything
-    c->prec == PGJ_FP32 ? run_green<float>(c, c->L, A, s) : run_green<double>(c, c->L, A, s);
+    c->prec == PGJ_FP32 ? run_green<float>(c, c->lpd, A, s) : run_green<double>(c, c->lpd, A, s);
   for (const FFTGeom& g : cands) {
     c->fg = g;
     A.geo = g;
-    int st = c->prec == PGJ_FP32 ? run_green<float>(c, c->L, A, s) : run_green<double>(c, c->L, A, s);
+    int st = c->prec == PGJ_FP32 ? run_green<float>(c, c->lpd, A, s) : run_green<double>(c, c->lpd, A, s);
     if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); c->fg = best; return st; }
     float ms = 1e30f;
     for (int trial = 0; trial < 2; ++trial) {  // best of two trials of three applies
       cudaEventRecord(e0, s);
       for (int r = 0; r < 3; ++r)
-        c->prec == PGJ_FP32 ? run_green<float>(c, c->L, A, s) : run_green<double>(c, c->L, A, s);
+        c->prec == PGJ_FP32 ? run_green<float>(c, c->lpd, A, s) : run_green<double>(c, c->lpd, A, s);
       cudaEventRecord(e1, s);
       cudaEventSynchronize(e1);
       float t = 0.f;

@@ -45,7 +45,8 @@ enum StencilMode { kPlain = 0, kPCG = 1, kResidual = 2 };
 
 struct StencilArgs {
   int n, ty, zc;
-  const double* a;
+  int lpd;                     // loads per design: load l reads the density of design l / lpd
+  const double* a;             // (designs, N)
   const void* in;
   void* out;
   const double* f;             // residual mode: right-hand side
@@ -80,6 +81,7 @@ struct Graphs;
 
 struct pgj_ctx {
   int n, L, prec;
+  int D, lpd;          // designs and loads per design (L = D * lpd); a plain context has D = 1
   double lam, mu;
   long long N;
   int ns;
@@ -91,10 +93,10 @@ struct pgj_ctx {
   pgj::Layout lay;
   char* base;
   size_t bytes;
-  // workspace views
-  double* a;
-  double* scale;
-  float* scale32;      // FP32 contexts: (3, N) component-planar FP32 copy of scale (first direction)
+  // workspace views (per-design fields are D consecutive blocks)
+  double* a;           // (D, N)
+  double* scale;       // (D, 3N)
+  float* scale32;      // FP32 contexts: (D, 3, N) component-planar FP32 copy of scale (first direction)
   double* symbol;
   float* symbol32;
   void* tw;            // n complex twiddles: double2[n] then float2[n]
@@ -106,7 +108,7 @@ struct pgj_ctx {
   void* q;             // (L, 3N) T
   void* sw;            // (L, 3N) T  s . w (unprojected preconditioned residual)
   void* spec;          // (L, 3, n, n, nsp) complex T
-  void* shat;          // (3, n, n, nsp) complex T: DFT of each component of the scale field
+  void* shat;          // (D, 3, n, n, nsp) complex T: DFT of each component of the scale field
   int fused;           // PCG iteration as operator + slab-fused update/transform kernels
   double* partials;    // (L, kPartialQ * kMaxPartials)
   pgj::LoadScalars* scal;  // L records used by the kernels being launched (outer or inner)
@@ -121,11 +123,14 @@ struct pgj_ctx {
   double inner_rtol;
   double rel_delta2;   // mixed reliable updates: replace r when ||r||^2 < rel_delta2 * anchor (0 = off)
   int mixed_mode;      // 0 reliable-update CG, 1 restarted refinement sweeps
+  int op64;            // FP32 contexts: the recurrence operator computes in FP64 (FP32 vectors)
+  int cap;             // per-load PCG iteration cap (4000, the reference's, unless set)
   int last_refinements;
   int pending_loads;       // loads of the solve enqueued by pgj_solve_async
   int diag_staged;         // stiffness-diagonal constants copied to aux
   int staged_loads;        // macros already on the device
-  double staged_macros[6 * 8];
+  double staged_macros[6 * pgj::kMaxTotalLoads];
+  double alphas[pgj::kMaxDesigns];  // alpha of each design's scale field
   long long last_launches;
   pgj::Graphs* graphs;
 };
@@ -175,7 +180,19 @@ int launch_rel_fold(pgj_ctx* c, int loads, bool all, cudaStream_t s);
 int launch_rel_sync(pgj_ctx* c, int loads, cudaStream_t s);
 // energy (pgj_energy.cu)
 int launch_energies(pgj_ctx* c, int loads, const double* u, const double* macros_dev, double* e, cudaStream_t s);
-int launch_effective_tensor(pgj_ctx* c, const double* u, double* C, double* e, cudaStream_t s);
+int launch_effective_tensor(pgj_ctx* c, const double* a, const double* u, double* C, double* e, cudaStream_t s);
+
+// Points the context's per-design views (a, scale, scale32, shat) at design d for the lifetime of
+// the scope, so that the single-design launchers (scale build, FP32 scale copy, DFT(s)) run on it.
+struct DesignScope {
+  pgj_ctx* c;
+  double* a;
+  double* scale;
+  float* scale32;
+  void* shat;
+  DesignScope(pgj_ctx* ctx, int d);
+  ~DesignScope();
+};
 
 int set_cuda_error(cudaError_t e);
 // one-time kernel attributes (dynamic shared memory limits); called at context creation

@@ -35,32 +35,51 @@ __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_grou
 __device__ __forceinline__ void cp_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
 // The rows of one plane issued by the lanes of one warp in parallel (lane r: rows r, r+32, ...):
-// lane 0 arms the mbarrier for all rows first. Called by all 32 lanes of the warp.
+// lane 0 arms the mbarrier for all rows first. Called by all 32 lanes of the warp. A node row is 3n
+// values: one copy of the interleaved row (cstride 0), or, for component-planar vectors (components
+// cstride apart in global memory), three copies of n values that land as [x components][y][z] rows.
 template <typename T>
 __device__ __forceinline__ void tma_plane_warp(T* buf, const T* in, int pz, int y0, int rows, int n, uint64_t* bar,
-                                               int lane) {
+                                               int lane, size_t cstride) {
   const unsigned rowbytes = unsigned(3 * n * sizeof(T));
   if (lane == 0) {
     fence_proxy_async();
     mbar_expect_tx(bar, rowbytes * rows);
   }
   __syncwarp();
-  for (int r = lane; r < rows; r += 32) {
-    int y = (y0 - 1 + r) % n;
-    if (y < 0) y += n;
-    tma_row(buf + r * 3 * n, in + (size_t(pz) * n + y) * size_t(3 * n), rowbytes, bar);
+  if (cstride == 0) {
+    for (int r = lane; r < rows; r += 32) {
+      int y = (y0 - 1 + r) % n;
+      if (y < 0) y += n;
+      tma_row(buf + r * 3 * n, in + (size_t(pz) * n + y) * size_t(3 * n), rowbytes, bar);
+    }
+  } else {
+    const unsigned cbytes = unsigned(n * sizeof(T));
+    for (int k = lane; k < 3 * rows; k += 32) {
+      const int r = k / 3, c = k - 3 * r;
+      int y = (y0 - 1 + r) % n;
+      if (y < 0) y += n;
+      tma_row(buf + (r * 3 + c) * n, in + c * cstride + (size_t(pz) * n + y) * size_t(n), cbytes, bar);
+    }
   }
 }
 
 template <typename T>
-__device__ __forceinline__ void tma_plane(T* buf, const T* in, int pz, int y0, int rows, int n, uint64_t* bar) {
+__device__ __forceinline__ void tma_plane(T* buf, const T* in, int pz, int y0, int rows, int n, uint64_t* bar,
+                                          size_t cstride) {
   const unsigned rowbytes = unsigned(3 * n * sizeof(T));
   fence_proxy_async();
   mbar_expect_tx(bar, rowbytes * rows);
   for (int r = 0; r < rows; ++r) {
     int y = (y0 - 1 + r) % n;
     if (y < 0) y += n;
-    tma_row(buf + r * 3 * n, in + (size_t(pz) * n + y) * size_t(3 * n), rowbytes, bar);
+    if (cstride == 0) {
+      tma_row(buf + r * 3 * n, in + (size_t(pz) * n + y) * size_t(3 * n), rowbytes, bar);
+    } else {
+      for (int c = 0; c < 3; ++c)
+        tma_row(buf + (r * 3 + c) * n, in + c * cstride + (size_t(pz) * n + y) * size_t(n),
+                unsigned(n * sizeof(T)), bar);
+    }
   }
 }
 
@@ -113,7 +132,8 @@ StencilGeom stencil_geom(int n, int loads) {
 }
 
 template <typename T>
-__device__ __forceinline__ void stage_plane(T* buf, const T* in, int pz, int y0, int rows, int n, int tid, int nthr) {
+__device__ __forceinline__ void stage_plane(T* buf, const T* in, int pz, int y0, int rows, int n, int tid, int nthr,
+                                            size_t cstride) {
   const int rowlen = 3 * n;
   const int total = rows * rowlen;
   for (int i = tid; i < total; i += nthr) {
@@ -121,7 +141,12 @@ __device__ __forceinline__ void stage_plane(T* buf, const T* in, int pz, int y0,
     const int rem = i - row * rowlen;
     int y = (y0 - 1 + row) % n;
     if (y < 0) y += n;
-    cp_async(buf + i, in + (size_t(pz) * n + y) * size_t(rowlen) + rem);
+    if (cstride == 0) {
+      cp_async(buf + i, in + (size_t(pz) * n + y) * size_t(rowlen) + rem);
+    } else {  // component-planar: buffer row = [component][x]
+      const int c = rem / n, x = rem - c * n;
+      cp_async(buf + i, in + c * cstride + (size_t(pz) * n + y) * size_t(n) + x);
+    }
   }
   cp_commit();
 }
@@ -156,13 +181,20 @@ struct Tri<float> {
 
 // Read the 4 nodes of the face (x..x+1, row..row+1) from a staged plane and form the face modes
 // F[f], f = mx + 2 my: F[0] = sum, F[1] = x-difference, F[2] = y-difference, F[3] = both.
-template <typename T>
+// PL: the staged rows are component-planar ([component][x]) instead of interleaved ([x][component]).
+template <bool PL, typename T>
+__device__ __forceinline__ Tri<T> node_at(const T* row, int x, int n) {
+  if constexpr (PL) return Tri<T>::make(row[x], row[n + x], row[2 * n + x]);
+  else return Tri<T>::load(row + 3 * x);
+}
+
+template <bool PL, typename T>
 __device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, Tri<T> (&F)[4], Tri<T>& own) {
   const int xp = (x + 1 == n) ? 0 : x + 1;
   const T* r0 = buf + row * 3 * n;
   const T* r1 = r0 + 3 * n;
-  const Tri<T> u00 = Tri<T>::load(r0 + 3 * x), u10 = Tri<T>::load(r0 + 3 * xp);
-  const Tri<T> u01 = Tri<T>::load(r1 + 3 * x), u11 = Tri<T>::load(r1 + 3 * xp);
+  const Tri<T> u00 = node_at<PL>(r0, x, n), u10 = node_at<PL>(r0, xp, n);
+  const Tri<T> u01 = node_at<PL>(r1, x, n), u11 = node_at<PL>(r1, xp, n);
   own = u00;
   const Tri<T> sx0 = u10 + u00, dx0 = u10 - u00, sx1 = u11 + u01, dx1 = u11 - u01;
   F[0] = sx1 + sx0;
@@ -171,17 +203,20 @@ __device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, 
   F[3] = dx1 - dx0;
 }
 
-// The same face modes one component at a time (the FP64 loop).
-template <typename T>
-__device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, T (&F)[4][3], T (&own)[3]) {
+// The same face modes one component at a time (the FP64 loop), in the compute type R (the staged
+// values are of the storage type T: FP64, or FP32 for the FP64-arithmetic form of the FP32 operator).
+template <bool PL, typename T, typename R>
+__device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, R (&F)[4][3], R (&own)[3]) {
   const int xp = (x + 1 == n) ? 0 : x + 1;
   const T* r0 = buf + row * 3 * n;
   const T* r1 = r0 + 3 * n;
+  const int xs = PL ? 1 : 3, cs = PL ? n : 1;  // element strides of x and of the component
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const T u00 = r0[3 * x + c], u10 = r0[3 * xp + c], u01 = r1[3 * x + c], u11 = r1[3 * xp + c];
+    const R u00 = R(r0[xs * x + cs * c]), u10 = R(r0[xs * xp + cs * c]), u01 = R(r1[xs * x + cs * c]),
+            u11 = R(r1[xs * xp + cs * c]);
     own[c] = u00;
-    const T sx0 = u10 + u00, dx0 = u10 - u00, sx1 = u11 + u01, dx1 = u11 - u01;
+    const R sx0 = u10 + u00, dx0 = u10 - u00, sx1 = u11 + u01, dx1 = u11 - u01;
     F[0][c] = sx1 + sx0;
     F[1][c] = dx1 + dx0;
     F[2][c] = sx1 - sx0;
@@ -190,8 +225,13 @@ __device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, 
 }
 
 // OCC = 1: blocks of up to 512 threads, registers unconstrained (128); OCC = 3: blocks of at most
-// 256 threads, three resident per SM (85 registers).
-template <typename T, int MODE, int OCC>
+// 256 threads, three resident per SM (85 registers). T is the storage type of p and q, R the
+// arithmetic type (R = double with T = float: FP32 vectors, FP64 element actions and node sums, for
+// high-contrast designs whose FP32 node sums cancel).
+//
+// PL: p and q of this launch are component-planar, (3, N) per load (the FP32 recurrence vectors of a
+// slab-fused mixed context); otherwise node-major with the components interleaved.
+template <typename T, int MODE, int OCC, typename R = T, bool PL = false>
 __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const StencilArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   const int n = A.n, TY = A.ty;
@@ -200,6 +240,7 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   const int load = blockIdx.z;
   const int nblk = gridDim.x * gridDim.y, blk = blockIdx.x + gridDim.x * blockIdx.y;
   const size_t N = size_t(n) * n * n;
+  const size_t cs = PL ? N : 0;  // global distance between the components of a node (0: interleaved)
   const int y0 = blockIdx.x * TY, z0 = blockIdx.y * A.zc;
   const int zc = min(A.zc, n - z0);
   const int ey = y0 - 1 + ty;
@@ -210,6 +251,8 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   if (MODE == kPCG) act = A.scal[load].active != 0;
   else if (A.active_ext) act = A.active_ext[load] != 0;
   else if (MODE == kResidual && A.rel_flags) act = A.rel_flags[load].reliable != 0;
+  // certification of a batched context: a design that took its last attempt keeps its certificate
+  if (MODE == kResidual && A.scal[load].frozen) act = false;
   T* out = reinterpret_cast<T*>(A.out) + size_t(load) * 3 * N;
   if (!act) {
     if (MODE == kPlain && out_row) {
@@ -228,8 +271,9 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   const int planevals = (TY + 2) * 3 * n;
   const int nt = n * (TY + 1);
   T* bufs = reinterpret_cast<T*>(smem_raw);
-  // corner exchange, double-buffered by step parity: [parity][corner 10 / 01 / 11][thread][3]
-  T* xch = bufs + NS * planevals;
+  // corner exchange in the arithmetic type, double-buffered by step parity:
+  // [parity][corner 10 / 01 / 11][thread][3] (n is even, so the plane buffers end 8-byte aligned)
+  R* xch = reinterpret_cast<R*>(bufs + NS * planevals);
   const int xsz = 3 * nt * 3;
   double* red = reinterpret_cast<double*>(xch + 2 * xsz + 2);  // 32 * 4, 16-byte padded
   red = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(red) + 15) & ~uintptr_t(15));
@@ -247,36 +291,36 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
     __syncthreads();
     if (tid == 0)
       for (int j = 0; j < NS && j < nplanes; ++j)
-        tma_plane(bufs + j * planevals, in, (z0 - 1 + j + n) % n, y0, TY + 2, n, &bars[j]);
+        tma_plane(bufs + j * planevals, in, (z0 - 1 + j + n) % n, y0, TY + 2, n, &bars[j], cs);
     bad = !mbar_wait(&bars[0], 0);  // every thread observes the arrival (acquire)
   } else {
-    stage_plane(bufs, in, (z0 - 1 + n) % n, y0, TY + 2, n, tid, nthr);
-    stage_plane(bufs + planevals, in, z0 % n, y0, TY + 2, n, tid, nthr);
+    stage_plane(bufs, in, (z0 - 1 + n) % n, y0, TY + 2, n, tid, nthr, cs);
+    stage_plane(bufs + planevals, in, z0 % n, y0, TY + 2, n, tid, nthr, cs);
     cp_wait_one();
     __syncthreads();
   }
   double acc[4] = {0.0, 0.0, 0.0, 0.0};
-  if constexpr (sizeof(T) == 4) {
+  if constexpr (sizeof(R) == 4) {
     // FP32: packed-pair arithmetic (Tri) and two z-steps per loop trip, which removes the copies of
     // the carried face modes; 47 vs 51 us at n = 64, 6 loads. FP64 keeps the one-step form below:
     // the same restructuring made it slower (64 vs 61 us).
     // lower-face modes, upper-plane carry and own node value of the plane below, in two sets that
     // swap roles every z-step (no copies at the loop edge)
     Tri<T> FA[4], UA[4], ownA, FB[4], UB[4], ownB;
-    face_modes(bufs, ty, tx, n, FA, ownB);
+    face_modes<PL>(bufs, ty, tx, n, FA, ownB);
     if (tma) {
       // buffer 0 is free once every thread has read plane 0
       if (__syncthreads_or(bad)) {
         if (tid == 0 && A.err) atomicExch(A.err, 1);
         return;
       }
-      if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0]);
+      if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0], cs);
     }
 #pragma unroll
     for (int f = 0; f < 4; ++f) UA[f] = Tri<T>::make(T(0), T(0), T(0));
     ownA = Tri<T>::make(T(0), T(0), T(0));
 
-    const double* aa = A.a;
+    const double* aa = A.a + size_t(load / A.lpd) * N;  // this load's design
 
     // element densities are read one plane ahead so their latency overlaps the previous plane
     const double* arow = aa + size_t(eyw) * n + tx;
@@ -311,10 +355,10 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
       } else {
         cp_wait_all();
         __syncthreads();
-        if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
+        if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr, cs);
       }
 
-      face_modes(cur, ty, tx, n, F1, own1);
+      face_modes<PL>(cur, ty, tx, n, F1, own1);
       // element modes: z level
       T Q[8][3];
 #pragma unroll
@@ -355,9 +399,9 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
         // warp 0 refills (its lanes issue the rows in parallel); a block of fewer than 32 threads
         // has no full warp, and thread 0 issues the rows alone
         if (full_warp0) {
-          if (tid < 32) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid);
+          if (tid < 32) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid, cs);
         } else if (tid == 0) {
-          tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb]);
+          tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb], cs);
         }
       }
       if (++jb == NS) { jb = 0; jpar ^= 1u; }
@@ -366,7 +410,7 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
         const Tri<T> qx = ((c00 + Tri<T>::load(xb + (0 * nt + tl) * 3)) + Tri<T>::load(xb + (1 * nt + tb) * 3)) +
                           Tri<T>::load(xb + (2 * nt + tbl) * 3);
         const size_t node = (size_t(ez) * n + ey) * n + tx;
-        T* o = out + 3 * node;
+        T* o = out + (PL ? node : 3 * node);
         // FP32 never runs the residual mode (the host rejects it); the branch is kept because the
         // build without it allocates registers differently and measured 0.6 us slower
         if (MODE == kResidual) {
@@ -379,7 +423,11 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
             acc[1 + c] += rv;
           }
         } else {
-          qx.store(o);
+          if constexpr (PL) {
+            o[0] = qx.get(0); o[N] = qx.get(1); o[2 * N] = qx.get(2);
+          } else {
+            qx.store(o);
+          }
           if (MODE == kPCG) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) acc[0] += double(own0.get(c)) * double(qx.get(c));
@@ -395,25 +443,25 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
       if (!step(s + 1, FB, UB, ownB, FA, UA, ownA)) return;
     }
   } else {
-    T F0[4][3], own[3], dummy[3];
-    face_modes(bufs, ty, tx, n, F0, dummy);
+    R F0[4][3], own[3], dummy[3];
+    face_modes<PL>(bufs, ty, tx, n, F0, dummy);
     if (tma) {
       // buffer 0 is free once every thread has read plane 0
       if (__syncthreads_or(bad)) {
         if (tid == 0 && A.err) atomicExch(A.err, 1);
         return;
       }
-      if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0]);
+      if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0], cs);
     }
-    T Up[4][3];
+    R Up[4][3];
 #pragma unroll
     for (int f = 0; f < 4; ++f)
 #pragma unroll
-      for (int c = 0; c < 3; ++c) Up[f][c] = T(0);
+      for (int c = 0; c < 3; ++c) Up[f][c] = R(0);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) own[c] = T(0);
+    for (int c = 0; c < 3; ++c) own[c] = R(0);
 
-    const double* aa = A.a;
+    const double* aa = A.a + size_t(load / A.lpd) * N;  // this load's design
 
     // element densities are read one plane ahead so their latency overlaps the previous plane
     const double* arow = aa + size_t(eyw) * n + tx;
@@ -432,7 +480,7 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
     const int tme = ty * n + tx;
     for (int s = 0; s <= zc; ++s) {
       const int ez = z0 - 1 + s;           // element plane
-      const T ae = T(a_next);
+      const R ae = R(a_next);
       if (s < zc) {
         za = za + 1 == n ? 0 : za + 1;
         a_next = __ldg(arow + size_t(za) * aplane);
@@ -443,13 +491,13 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
       } else {
         cp_wait_all();
         __syncthreads();
-        if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
+        if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr, cs);
       }
 
-      T F1[4][3], own1[3];
-      face_modes(cur, ty, tx, n, F1, own1);
+      R F1[4][3], own1[3];
+      face_modes<PL>(cur, ty, tx, n, F1, own1);
       // element modes: z level
-      T Q[8][3];
+      R Q[8][3];
 #pragma unroll
       for (int f = 0; f < 4; ++f)
 #pragma unroll
@@ -457,10 +505,10 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
           Q[f][c] = F1[f][c] + F0[f][c];
           Q[f + 4][c] = F1[f][c] - F0[f][c];
         }
-      T P[8][3];
-      element_modal<T>(Q, ae, A.kc, P);
+      R P[8][3];
+      element_modal<R>(Q, ae, A.kc, P);
       // z-level transpose: U -> upper plane (ez+1), G -> lower plane (ez)
-      T U[4][3], G[4][3];
+      R U[4][3], G[4][3];
 #pragma unroll
       for (int f = 0; f < 4; ++f)
 #pragma unroll
@@ -470,13 +518,13 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
         }
       // lower face of the element (node plane ez) as its four corner nodes: this thread keeps the
       // (x, y) corner and hands (x+1, y), (x, y+1), (x+1, y+1) to their owners through shared memory
-      T c00[3];
-      T* xb = xch + (s & 1) * xsz;
+      R c00[3];
+      R* xb = xch + (s & 1) * xsz;
       if (s >= 1) {
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-          const T ly0 = G[0][c] - G[2][c], ly1 = G[1][c] - G[3][c];
-          const T uy0 = G[0][c] + G[2][c], uy1 = G[1][c] + G[3][c];
+          const R ly0 = G[0][c] - G[2][c], ly1 = G[1][c] - G[3][c];
+          const R uy0 = G[0][c] + G[2][c], uy1 = G[1][c] + G[3][c];
           c00[c] = ly0 - ly1;
           xb[(0 * nt + tme) * 3 + c] = ly0 + ly1;
           xb[(1 * nt + tme) * 3 + c] = uy0 - uy1;
@@ -492,20 +540,20 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
         // warp 0 refills (its lanes issue the rows in parallel); a block of fewer than 32 threads
         // has no full warp, and thread 0 issues the rows alone
         if (full_warp0) {
-          if (tid < 32) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid);
+          if (tid < 32) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid, cs);
         } else if (tid == 0) {
-          tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb]);
+          tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb], cs);
         }
       }
       if (++jb == NS) { jb = 0; jpar ^= 1u; }
       zr = zr + 1 == n ? 0 : zr + 1;
       if (s >= 1 && out_row) {
-        T qx[3];
+        R qx[3];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
           qx[c] = ((c00[c] + xb[(0 * nt + tl) * 3 + c]) + xb[(1 * nt + tb) * 3 + c]) + xb[(2 * nt + tbl) * 3 + c];
         const size_t node = (size_t(ez) * n + ey) * n + tx;
-        T* o = out + 3 * node;
+        T* o = out + (PL ? node : 3 * node);
         if (MODE == kResidual) {
           const double* fl = A.f + size_t(load) * 3 * N + 3 * node;
 #pragma unroll
@@ -517,7 +565,7 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
           }
         } else {
 #pragma unroll
-          for (int c = 0; c < 3; ++c) o[c] = qx[c];
+          for (int c = 0; c < 3; ++c) o[PL ? c * N : c] = T(qx[c]);
           if (MODE == kPCG) {
 #pragma unroll
             for (int c = 0; c < 3; ++c) acc[0] += double(own[c]) * double(qx[c]);
@@ -567,15 +615,16 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   }
 }
 
-// Tile autotuner: times the operator (all loads, plain mode) for candidate tile shapes on the
-// context's own buffers and keeps the fastest. Results are cached per (n, loads, precision) for the
-// process, so contexts created later reuse the choice.
+// Tile autotuner: times the operator (the loads of one design, plain mode) for candidate tile shapes
+// on the context's own buffers and keeps the fastest. Results are cached per (n, loads per design,
+// precision) for the process, so contexts created later, batched ones included, reuse the choice
+// (and with it the order of the operator's block partial sums).
 static std::mutex g_tune_mutex;
 static std::map<std::tuple<int, int, int>, StencilGeom> g_tuned;
 
 int autotune_stencil(pgj_ctx* c, cudaStream_t s) {
   const int n = c->n;
-  const auto key = std::make_tuple(n, c->L, c->prec);
+  const auto key = std::make_tuple(n, c->lpd, c->prec);
   {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     auto it = g_tuned.find(key);
@@ -598,7 +647,7 @@ int autotune_stencil(pgj_ctx* c, cudaStream_t s) {
   const void* in = c->p;
   void* out = c->q;
   // bring the clocks up before timing anything
-  for (int r = 0; r < 30; ++r) launch_stencil(c, kPlain, c->L, c->prec, in, out, nullptr, nullptr, s);
+  for (int r = 0; r < 30; ++r) launch_stencil(c, kPlain, c->lpd, c->prec, in, out, nullptr, nullptr, s);
   for (int ty : tys)
     for (int zc : zcs)
       for (int occ : {1, 3})
@@ -607,12 +656,12 @@ int autotune_stencil(pgj_ctx* c, cudaStream_t s) {
         StencilGeom g = stencil_geom_shape(n, ty, zc, stages, occ);
         if (g.ntiles * g.nchunks > kMaxPartials) continue;
         c->sg = g;
-        int st = launch_stencil(c, kPlain, c->L, c->prec, in, out, nullptr, nullptr, s);  // warm
+        int st = launch_stencil(c, kPlain, c->lpd, c->prec, in, out, nullptr, nullptr, s);  // warm
         if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
         float ms = 1e30f;
         for (int trial = 0; trial < 2; ++trial) {  // best of two trials of five launches
           cudaEventRecord(e0, s);
-          for (int r = 0; r < 5; ++r) launch_stencil(c, kPlain, c->L, c->prec, in, out, nullptr, nullptr, s);
+          for (int r = 0; r < 5; ++r) launch_stencil(c, kPlain, c->lpd, c->prec, in, out, nullptr, nullptr, s);
           cudaEventRecord(e1, s);
           cudaEventSynchronize(e1);
           float t = 0.f;
@@ -655,6 +704,9 @@ static void set_stencil_smem(int lim) {
   cudaFuncSetAttribute(k_stencil<double, kPlain, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_stencil<double, kPCG, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_stencil<double, kResidual, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<float, kPCG, OCC, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<float, kPCG, OCC, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<float, kPCG, OCC, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 
 int prepare_stencil_kernels() {
@@ -664,10 +716,13 @@ int prepare_stencil_kernels() {
 }
 
 template <int OCC>
-static void launch_stencil_kernel(int mode, int prec, dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                                  const StencilArgs& A) {
+static void launch_stencil_kernel(int mode, int prec, bool r64, bool planar, dim3 grid, dim3 block, size_t smem,
+                                  cudaStream_t s, const StencilArgs& A) {
   if (prec == PGJ_FP32) {
     if (mode == kPlain) k_stencil<float, kPlain, OCC><<<grid, block, smem, s>>>(A);
+    else if (planar && r64) k_stencil<float, kPCG, OCC, double, true><<<grid, block, smem, s>>>(A);
+    else if (planar) k_stencil<float, kPCG, OCC, float, true><<<grid, block, smem, s>>>(A);
+    else if (r64) k_stencil<float, kPCG, OCC, double><<<grid, block, smem, s>>>(A);
     else k_stencil<float, kPCG, OCC><<<grid, block, smem, s>>>(A);
   } else {
     if (mode == kPlain) k_stencil<double, kPlain, OCC><<<grid, block, smem, s>>>(A);
@@ -681,35 +736,44 @@ int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, vo
   const int n = c->n;
   StencilArgs A;
   A.n = n; A.ty = c->sg.ty; A.zc = c->sg.zc;
+  A.lpd = c->lpd;
   A.a = c->a; A.in = in; A.out = out; A.f = f; A.active_ext = active_ext;
-  A.scal = c->scal; A.partials = c->partials; A.kc = c->kc; A.iteration_cap = 4000;
+  A.scal = c->scal; A.partials = c->partials; A.kc = c->kc; A.iteration_cap = c->cap;
   A.err = c->cond + 2;
   A.rel_flags = rel_flags;
   const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
+  // the FP32 recurrence vectors of a slab-fused context are component-planar, (3, N) per load
+  const bool planar = prec == PGJ_FP32 && mode == kPCG && c->fused;
   // TMA rows need 16-byte aligned starts and sizes: (3 n * element size) % 16 == 0 and an aligned base
-  A.tma = ((3 * size_t(n) * tsz) % 16 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0) ? 1 : 0;
+  // (component-planar rows: n * element size, the component blocks 4 n^3 bytes apart)
+  const size_t rowb = (planar ? 1 : 3) * size_t(n) * tsz;
+  A.tma = (rowb % 16 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0) ? 1 : 0;
   dim3 grid(c->sg.ntiles, c->sg.nchunks, loads), block(n, c->sg.ty + 1);
   A.stages = A.tma ? c->sg.stages : 2;
-  const size_t smem = tsz * (size_t(A.stages) * (c->sg.ty + 2) * 3 * n + size_t(2) * 9 * (c->sg.ty + 1) * n) +
+  // FP32 recurrence operator with FP64 arithmetic (high-contrast mixed solves)
+  const bool r64 = prec == PGJ_FP32 && mode == kPCG && c->op64;
+  const size_t rsz = r64 ? 8 : tsz;  // corner exchange in the arithmetic type
+  const size_t smem = tsz * size_t(A.stages) * (c->sg.ty + 2) * 3 * n + rsz * size_t(2) * 9 * (c->sg.ty + 1) * n +
                       32 * 4 * 8 + 16 + 8 * A.stages + 64;
   if (c->sg.ntiles * c->sg.nchunks > kMaxPartials) return PGJ_ERR_UNSUPPORTED;
   if (mode != kPlain && mode != kPCG && !(mode == kResidual && prec == PGJ_FP64)) return PGJ_ERR_ARGUMENT;
   // the occupancy variant applies to the recurrence operator; the residual keeps the wide form
   const bool occ3 = c->sg.occ == 3 && mode != kResidual && n * (c->sg.ty + 1) <= 256 && smem <= 72 * 1024;
-  if (occ3) launch_stencil_kernel<3>(mode, prec, grid, block, smem, s, A);
-  else launch_stencil_kernel<1>(mode, prec, grid, block, smem, s, A);
+  if (occ3) launch_stencil_kernel<3>(mode, prec, r64, planar, grid, block, smem, s, A);
+  else launch_stencil_kernel<1>(mode, prec, r64, planar, grid, block, smem, s, A);
   return check_launch();
 }
 
 // --------------------------------------------------------------------------- right-hand side
 // f(node) = -V sum over the 8 elements e = node - b of B_c(b)^T (a_e C0 eps), B_c the element-centre
 // gradient (+-1/(4h) per axis); same arithmetic as hybrid_kernels.cu:50-68.
-__global__ void k_rhs(int n, int loads, const double* __restrict__ a, const double* __restrict__ macros,
+__global__ void k_rhs(int n, int loads, int lpd, const double* __restrict__ a, const double* __restrict__ macros,
                       double lam, double mu, double* __restrict__ f) {
   const size_t N = size_t(n) * n * n;
   const size_t node = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int load = blockIdx.y;
   if (node >= N || load >= loads) return;
+  a += size_t(load / lpd) * N;  // this load's design
   const int x = int(node % n), y = int((node / n) % n), z = int(node / (size_t(n) * n));
   const double* m = macros + 6 * load;
   // C0 eps (Voigt, engineering shear)
@@ -740,7 +804,7 @@ __global__ void k_rhs(int n, int loads, const double* __restrict__ a, const doub
 int launch_rhs(pgj_ctx* c, int loads, const double* macros_dev, double* f, cudaStream_t s) {
   const size_t N = size_t(c->N);
   dim3 grid(unsigned((N + 255) / 256), loads);
-  k_rhs<<<grid, 256, 0, s>>>(c->n, loads, c->a, macros_dev, c->lam, c->mu, f);
+  k_rhs<<<grid, 256, 0, s>>>(c->n, loads, c->lpd, c->a, macros_dev, c->lam, c->mu, f);
   return check_launch();
 }
 
@@ -775,6 +839,8 @@ __global__ void k_norms(int n, const double* __restrict__ f, double rtol, LoadSc
       S.bad = 0;
       S.failed = 0;
       S.active = 0;
+      S.frozen = 0;
+      S.restarts = 0;
     }
   }
 }
@@ -790,6 +856,7 @@ int launch_norms(pgj_ctx* c, int loads, const double* f, double rtol, cudaStream
 __global__ void k_mean3(int n, const double* __restrict__ u, int which, LoadScalars* scal, double* partials) {
   const size_t N = size_t(n) * n * n;
   const int load = blockIdx.y;
+  if (which == 0 && scal[load].frozen) return;  // certification of a design that took its last attempt
   const double* ul = u + size_t(load) * 3 * N;
   double acc[3] = {0.0, 0.0, 0.0};
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
@@ -815,6 +882,7 @@ __global__ void k_mean3(int n, const double* __restrict__ u, int which, LoadScal
 __global__ void k_sub_mean3(int n, double* __restrict__ u, const LoadScalars* scal) {
   const size_t N3 = 3 * size_t(n) * n * n;
   const int load = blockIdx.y;
+  if (scal[load].frozen) return;
   double* ul = u + size_t(load) * N3;
   const double m0 = scal[load].mean_u[0], m1 = scal[load].mean_u[1], m2 = scal[load].mean_u[2];
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x) {

@@ -117,27 +117,26 @@ int launch_update_ur(pgj_ctx* c, int loads, int prec, double* u64, void* uT, cud
     if (u64)
       k_update_ur<float, double><<<grid, 256, 0, s>>>(c->n, u64, static_cast<float*>(c->r),
                                                       static_cast<const float*>(c->p), static_cast<const float*>(c->q),
-                                                      c->scal, c->partials, 4000, rel);
+                                                      c->scal, c->partials, c->cap, rel);
     else
       k_update_ur<float, float><<<grid, 256, 0, s>>>(c->n, static_cast<float*>(uT), static_cast<float*>(c->r),
                                                      static_cast<const float*>(c->p), static_cast<const float*>(c->q),
-                                                     c->scal, c->partials, 4000, rel);
+                                                     c->scal, c->partials, c->cap, rel);
   } else {
     k_update_ur<double, double><<<grid, 256, 0, s>>>(c->n, u64 ? u64 : static_cast<double*>(uT),
                                                      static_cast<double*>(c->r), static_cast<const double*>(c->p),
-                                                     static_cast<const double*>(c->q), c->scal, c->partials, 4000, rel);
+                                                     static_cast<const double*>(c->q), c->scal, c->partials, c->cap, rel);
   }
   return check_launch();
 }
 
-// The loop body runs at most kMaxBodyRuns times per attempt whatever the masks say, so a graph
-// WHILE loop can never spin unbounded (the per-load cap of 4000 iterations ends it first).
-constexpr int kMaxBodyRuns = 4100;
+// The loop body runs at most `bound` (the iteration cap + 100) times per attempt whatever the masks
+// say, so a graph WHILE loop can never spin unbounded (the per-load iteration cap ends it first).
 
 template <typename T>
 __global__ void __launch_bounds__(256) k_update_p(int n, int loads, T* __restrict__ p, const T* __restrict__ sw,
                                                   const LoadScalars* scal, int init, cudaGraphConditionalHandle h,
-                                                  int set_cond, int* body_runs) {
+                                                  int set_cond, int* body_runs, int bound) {
   const size_t N3 = 3 * size_t(n) * n * n;
   const int load = blockIdx.y;
   if (set_cond && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) {
@@ -145,8 +144,8 @@ __global__ void __launch_bounds__(256) k_update_p(int n, int loads, T* __restric
     for (int l = 0; l < loads; ++l) any |= scal[l].active;
     const int runs = ++body_runs[0];
     body_runs[5] += 1;                             // loop bodies over the whole solve (launch accounting)
-    if (runs >= kMaxBodyRuns) body_runs[1] = 1;  // recorded: loop stopped by the bound
-    cudaGraphSetConditional(h, (any && runs < kMaxBodyRuns) ? 1u : 0u);
+    if (runs >= bound) body_runs[1] = 1;  // recorded: loop stopped by the bound
+    cudaGraphSetConditional(h, (any && runs < bound) ? 1u : 0u);
   }
   const LoadScalars& S = scal[load];
   if (!S.active) return;
@@ -176,37 +175,43 @@ int launch_update_p(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, 
   dim3 grid(update_blocks(c, prec), loads);
   if (prec == PGJ_FP32)
     k_update_p<float><<<grid, 256, 0, s>>>(c->n, loads, static_cast<float*>(c->p), static_cast<const float*>(c->sw),
-                                           c->scal, init ? 1 : 0, h, set_cond ? 1 : 0, c->cond);
+                                           c->scal, init ? 1 : 0, h, set_cond ? 1 : 0, c->cond, c->cap + 100);
   else
     k_update_p<double><<<grid, 256, 0, s>>>(c->n, loads, static_cast<double*>(c->p), static_cast<const double*>(c->sw),
-                                            c->scal, init ? 1 : 0, h, set_cond ? 1 : 0, c->cond);
+                                            c->scal, init ? 1 : 0, h, set_cond ? 1 : 0, c->cond, c->cap + 100);
   return check_launch();
 }
 
 // active = ||r||^2 > target^2 and iterations < cap and not bad (resident.py:120); also resets the
-// loop-body counter of the attempt.
+// loop-body counter of the attempt. Loads of a design that took its last attempt stay inactive.
 __global__ void k_init_mask(int loads, LoadScalars* scal, int cap, int* body_runs) {
-  const int l = threadIdx.x;
-  if (l == 0) body_runs[0] = 0;
-  if (l >= loads) return;
-  LoadScalars& S = scal[l];
-  S.active = (S.res2 > S.target2) && (S.iterations < cap) && !S.bad ? 1 : 0;
-  S.failed = 0;
+  if (threadIdx.x == 0) body_runs[0] = 0;
+  for (int l = threadIdx.x; l < loads; l += blockDim.x) {
+    LoadScalars& S = scal[l];
+    S.active = (S.res2 > S.target2) && (S.iterations < cap) && !S.bad && !S.frozen ? 1 : 0;
+    S.failed = 0;
+  }
 }
 
 int launch_init_mask(pgj_ctx* c, int loads, cudaStream_t s) {
-  k_init_mask<<<1, 32, 0, s>>>(loads, c->scal, 4000, c->cond);
+  k_init_mask<<<1, 32, 0, s>>>(loads, c->scal, c->cap, c->cond);
   return check_launch();
 }
 
 // ------------------------------------------------------------------------------ mixed refinement
 // Start of one refinement sweep, per load: the FP64 certificate decides whether the load still needs
 // a correction; r_in = T(r64), d = 0; the inner target is inner_rtol * ||r64||.
+// `planar`: the FP32 vectors r and d are component-planar, (3, N) per load (slab-fused contexts);
+// the FP64 vectors are node-major interleaved either way.
+__device__ __forceinline__ size_t pidx(size_t node, int c, size_t N, int planar) {
+  return planar ? size_t(c) * N + node : 3 * node + c;
+}
+
 template <typename T>
 __global__ void __launch_bounds__(256) k_inner_start(int n, const double* __restrict__ r64, T* __restrict__ r,
                                                      T* __restrict__ d, const LoadScalars* out_scal,
                                                      LoadScalars* in_scal, double* partials, double inner_rtol,
-                                                     int* body_runs) {
+                                                     int* body_runs, int planar) {
   const size_t N = size_t(n) * n * n, N3 = 3 * N;
   const int load = blockIdx.y;
   const LoadScalars& O = out_scal[load];
@@ -222,10 +227,10 @@ __global__ void __launch_bounds__(256) k_inner_start(int n, const double* __rest
   for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-      const size_t k = off + 3 * i + c;
+      const size_t k = off + 3 * i + c, kt = off + pidx(i, c, N, planar);
       const T v = T(r64[k]);
-      r[k] = v;
-      d[k] = T(0);
+      r[kt] = v;
+      d[kt] = T(0);
       const double dv = double(v);
       acc[0] += dv * dv;
       acc[1 + c] += dv;
@@ -257,14 +262,15 @@ __global__ void __launch_bounds__(256) k_inner_start(int n, const double* __rest
 // End of a sweep: x += d for touched loads; iteration and latch bookkeeping on the outer record.
 template <typename T>
 __global__ void __launch_bounds__(256) k_inner_finish(int n, double* __restrict__ x, const T* __restrict__ d,
-                                                      LoadScalars* out_scal, const LoadScalars* in_scal) {
-  const size_t N3 = 3 * size_t(n) * n * n;
+                                                      LoadScalars* out_scal, const LoadScalars* in_scal, int planar) {
+  const size_t N = size_t(n) * n * n, N3 = 3 * N;
   const int load = blockIdx.y;
   const LoadScalars& S = in_scal[load];
   if (!S.touched) return;
   const size_t off = size_t(load) * N3;
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x)
-    x[off + i] += double(d[off + i]);
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) x[off + 3 * i + c] += double(d[off + pidx(i, c, N, planar)]);
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     out_scal[load].total_iterations += S.iterations;
     out_scal[load].bad |= S.bad;
@@ -274,13 +280,14 @@ __global__ void __launch_bounds__(256) k_inner_finish(int n, double* __restrict_
 int launch_inner_start(pgj_ctx* c, int loads, double inner_rtol, cudaStream_t s) {
   dim3 grid(2 * 148, loads);
   k_inner_start<float><<<grid, 256, 0, s>>>(c->n, c->r64, static_cast<float*>(c->r), static_cast<float*>(c->d),
-                                            c->scal_out, c->scal_in, c->partials, inner_rtol, c->cond);
+                                            c->scal_out, c->scal_in, c->partials, inner_rtol, c->cond, c->fused);
   return check_launch();
 }
 
 int launch_inner_finish(pgj_ctx* c, int loads, cudaStream_t s) {
   dim3 grid(2 * 148, loads);
-  k_inner_finish<float><<<grid, 256, 0, s>>>(c->n, c->x, static_cast<const float*>(c->d), c->scal_out, c->scal_in);
+  k_inner_finish<float><<<grid, 256, 0, s>>>(c->n, c->x, static_cast<const float*>(c->d), c->scal_out, c->scal_in,
+                                             c->fused);
   return check_launch();
 }
 
@@ -292,14 +299,18 @@ int launch_inner_finish(pgj_ctx* c, int loads, cudaStream_t s) {
 template <typename T>
 __global__ void __launch_bounds__(256) k_rel_start(int n, const double* __restrict__ r64, T* __restrict__ r,
                                                    T* __restrict__ d, const LoadScalars* out, LoadScalars* in, int cap,
-                                                   int* body_runs) {
-  const size_t N3 = 3 * size_t(n) * n * n;
+                                                   int* body_runs, int planar) {
+  const size_t N = size_t(n) * n * n, N3 = 3 * N;
   const int load = blockIdx.y;
   if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) body_runs[0] = 0;
   const size_t off = size_t(load) * N3;
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x) {
-    r[off + i] = T(r64[off + i]);
-    d[off + i] = T(0);
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const size_t kt = off + pidx(i, c, N, planar);
+      r[kt] = T(r64[off + 3 * i + c]);
+      d[kt] = T(0);
+    }
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) {
     const LoadScalars& O = out[load];
@@ -312,7 +323,7 @@ __global__ void __launch_bounds__(256) k_rel_start(int n, const double* __restri
     S.bad = O.bad;
     S.failed = 0;
     S.reliable = 0;
-    S.active = (O.res2 > O.target2) && (O.iterations < cap) && !O.bad ? 1 : 0;
+    S.active = (O.res2 > O.target2) && (O.iterations < cap) && !O.bad && !O.frozen ? 1 : 0;
   }
 }
 
@@ -328,8 +339,8 @@ __global__ void k_rel_cond(int loads, const LoadScalars* in, cudaGraphConditiona
 // x += d, d = 0 for flagged loads (all loads when `all`)
 template <typename T>
 __global__ void __launch_bounds__(256) k_rel_fold(int n, double* __restrict__ x, T* __restrict__ d,
-                                                  const LoadScalars* in, LoadScalars* out, int all) {
-  const size_t N3 = 3 * size_t(n) * n * n;
+                                                  const LoadScalars* in, LoadScalars* out, int all, int planar) {
+  const size_t N = size_t(n) * n * n, N3 = 3 * N;
   const int load = blockIdx.y;
   if (!all && !in[load].reliable) return;
   if (all && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -338,9 +349,13 @@ __global__ void __launch_bounds__(256) k_rel_fold(int n, double* __restrict__ x,
     out[load].bad |= in[load].bad;
   }
   const size_t off = size_t(load) * N3;
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x) {
-    x[off + i] += double(d[off + i]);
-    d[off + i] = T(0);
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const size_t kt = off + pidx(i, c, N, planar);
+      x[off + 3 * i + c] += double(d[kt]);
+      d[kt] = T(0);
+    }
   }
 }
 
@@ -348,14 +363,15 @@ __global__ void __launch_bounds__(256) k_rel_fold(int n, double* __restrict__ x,
 // resets the recurrence scalars to it and decides whether the load keeps iterating
 template <typename T>
 __global__ void __launch_bounds__(256) k_rel_sync(int n, const double* __restrict__ r64, T* __restrict__ r,
-                                                  const LoadScalars* out, LoadScalars* in, int cap) {
-  const size_t N3 = 3 * size_t(n) * n * n;
+                                                  const LoadScalars* out, LoadScalars* in, int cap, int planar) {
+  const size_t N = size_t(n) * n * n, N3 = 3 * N;
   const int load = blockIdx.y;
   LoadScalars& S = in[load];
   if (!S.reliable) return;
   const size_t off = size_t(load) * N3;
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N3; i += size_t(gridDim.x) * blockDim.x)
-    r[off + i] = T(r64[off + i]);
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) r[off + pidx(i, c, N, planar)] = T(r64[off + 3 * i + c]);
   if (!last_block(&S.ticket[kTicketAux2], gridDim.x)) return;
   if (threadIdx.x == 0) {
     const LoadScalars& O = out[load];
@@ -367,33 +383,46 @@ __global__ void __launch_bounds__(256) k_rel_sync(int n, const double* __restric
   }
 }
 
-// Device-side restart decision after an attempt's certification (resident.py:202-205): another
-// attempt only when some certificate failed, fewer than two restarts were taken, no load latched
-// `bad`, no failing load reached the iteration cap and the loop bound was not hit.
-__global__ void k_decide(int loads, const LoadScalars* out, int* counters, cudaGraphConditionalHandle h, int cap) {
+// Device-side restart decision after an attempt's certification (resident.py:202-205), per design
+// (the loads [g lpd, (g+1) lpd) of a batched context; a plain context is one design): another
+// attempt only when some certificate of the design failed, fewer than two restarts were taken, none
+// of its loads latched `bad`, no failing load reached the iteration cap and the loop bound was not
+// hit. A design that stops is frozen: later attempts of its batch-mates leave its loads untouched.
+__global__ void k_decide(int loads, int lpd, LoadScalars* out, int* counters, cudaGraphConditionalHandle h,
+                         int cap) {
   if (threadIdx.x != 0) return;
-  bool all = true, anybad = false, capped = false;
-  for (int l = 0; l < loads; ++l) {
-    const LoadScalars& S = out[l];
-    const bool ok = isfinite(S.absolute) && S.absolute * S.absolute <= S.target2 && !S.bad;
-    all = all && ok;
-    anybad = anybad || S.bad;
-    capped = capped || (!ok && S.iterations >= cap);
+  bool any_again = false;
+  for (int g = 0; g * lpd < loads; ++g) {
+    bool all = true, anybad = false, capped = false;
+    const int l1 = min(loads, (g + 1) * lpd);
+    if (out[g * lpd].frozen) continue;
+    for (int l = g * lpd; l < l1; ++l) {
+      const LoadScalars& S = out[l];
+      const bool ok = isfinite(S.absolute) && S.absolute * S.absolute <= S.target2 && !S.bad;
+      all = all && ok;
+      anybad = anybad || S.bad;
+      capped = capped || (!ok && S.iterations >= cap);
+    }
+    const bool again = !all && out[g * lpd].restarts < 2 && !anybad && !capped && !counters[1] && !counters[2];
+    for (int l = g * lpd; l < l1; ++l) {
+      if (again) out[l].restarts += 1;
+      else out[l].frozen = 1;
+    }
+    any_again = any_again || again;
   }
-  const bool again = !all && counters[4] < 2 && !anybad && !capped && !counters[1] && !counters[2];
-  if (again) counters[4] += 1;
-  cudaGraphSetConditional(h, again ? 1u : 0u);
+  if (any_again) counters[4] += 1;  // attempts after the first, over the whole context
+  cudaGraphSetConditional(h, any_again ? 1u : 0u);
 }
 
 int launch_decide(pgj_ctx* c, int loads, cudaGraphConditionalHandle h, cudaStream_t s) {
-  k_decide<<<1, 32, 0, s>>>(loads, c->scal_out, c->cond, h, 4000);
+  k_decide<<<1, 32, 0, s>>>(loads, c->lpd, c->scal_out, c->cond, h, c->cap);
   return check_launch();
 }
 
 int launch_rel_start(pgj_ctx* c, int loads, cudaStream_t s) {
   k_rel_start<float><<<dim3(2 * 148, loads), 256, 0, s>>>(c->n, c->r64, static_cast<float*>(c->r),
-                                                          static_cast<float*>(c->d), c->scal_out, c->scal_in, 4000,
-                                                          c->cond);
+                                                          static_cast<float*>(c->d), c->scal_out, c->scal_in, c->cap,
+                                                          c->cond, c->fused);
   return check_launch();
 }
 int launch_rel_cond(pgj_ctx* c, int loads, cudaGraphConditionalHandle h, cudaStream_t s) {
@@ -402,12 +431,12 @@ int launch_rel_cond(pgj_ctx* c, int loads, cudaGraphConditionalHandle h, cudaStr
 }
 int launch_rel_fold(pgj_ctx* c, int loads, bool all, cudaStream_t s) {
   k_rel_fold<float><<<dim3(2 * 148, loads), 256, 0, s>>>(c->n, c->x, static_cast<float*>(c->d), c->scal_in,
-                                                         c->scal_out, all ? 1 : 0);
+                                                         c->scal_out, all ? 1 : 0, c->fused);
   return check_launch();
 }
 int launch_rel_sync(pgj_ctx* c, int loads, cudaStream_t s) {
   k_rel_sync<float><<<dim3(2 * 148, loads), 256, 0, s>>>(c->n, c->r64, static_cast<float*>(c->r), c->scal_out,
-                                                         c->scal_in, 4000);
+                                                         c->scal_in, c->cap, c->fused);
   return check_launch();
 }
 

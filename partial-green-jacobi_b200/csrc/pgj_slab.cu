@@ -33,8 +33,8 @@ struct SlabArgs {
   void* r;                // (L,3N) T recurrence residual
   void* u;                // (L,3N) U iterate (FP64 x, or the FP32 correction d)
   const double* r64;      // sync mode: FP64 true residual
-  const double* scale;    // (3N) FP64 scale field s
-  const float* scale32;   // FP32 contexts: (3, N) component-planar FP32 copy of s
+  const double* scale;    // (designs, 3N) FP64 scale field s
+  const float* scale32;   // FP32 contexts: (designs, 3, N) component-planar FP32 copy of s
   void* spec;             // (L,3,n,n,nsp) complex T
   const void* tw;         // n complex T twiddles
   LoadScalars* scal;      // recurrence records
@@ -43,13 +43,14 @@ struct SlabArgs {
   int cap;
   double rel_delta2;
   int loads;
+  int lpd;                // loads per design: load l uses the scale field of design l / lpd
   int init;               // ifxy: p = P(s.w) (first direction)
   int set_cond;           // ifxy: set the WHILE condition (any load active, bounded body count)
   cudaGraphConditionalHandle h;
   int* counters;
 };
 
-constexpr int kMaxBodyRunsSlab = 4100;  // same bound as the unfused loop body
+// the loop body runs at most cap + 100 times per attempt (the same bound as the unfused loop body)
 
 template <typename T>
 __device__ __forceinline__ T* real_view(cplx<T>* b) { return reinterpret_cast<T*>(b); }
@@ -104,10 +105,17 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   double* red = reinterpret_cast<double*>(b1 + size_t(n) * nsp);
   const size_t N = size_t(nn) * n, N3 = 3 * N;
   const size_t node0 = size_t(z) * nn;
-  const size_t off = size_t(load) * N3 + 3 * node0 + c;  // dof of node (0,0,z), component c
+  // FP32 recurrence vectors are component-planar, (3, N) per load: the slab's values are contiguous;
+  // FP64 vectors (and the FP64 true residual) keep the node-major interleaved layout
+  constexpr bool PL = sizeof(T) == 4;
+  constexpr int KS = PL ? 1 : 3;                           // element stride of consecutive nodes
+  const size_t off = PL ? size_t(load) * N3 + size_t(c) * N + node0
+                        : size_t(load) * N3 + 3 * node0 + c;  // dof of node (0,0,z), component c
+  const size_t off64 = size_t(load) * N3 + 3 * node0 + c;
   T* r = reinterpret_cast<T*>(A.r) + off;
-  const double* sc = A.scale + 3 * node0 + c;
-  const float* s32 = sizeof(T) == 4 ? A.scale32 + size_t(c) * nn * n + node0 : nullptr;  // coalesced
+  const size_t dsg = size_t(load / A.lpd);
+  const double* sc = A.scale + dsg * N3 + 3 * node0 + c;
+  const float* s32 = sizeof(T) == 4 ? A.scale32 + dsg * N3 + size_t(c) * nn * n + node0 : nullptr;  // coalesced
   T* packed = real_view<T>(b0);
   const int lpx = R64 ? kLine64 : n + 1;  // pitch of the packed x lines
   double acc[2] = {0.0, 0.0};
@@ -118,7 +126,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   const T* pg = reinterpret_cast<const T*>(A.p) + off;
   const T* qg = reinterpret_cast<const T*>(A.q) + off;
   U* ug = reinterpret_cast<U*>(A.u) + off;
-  const double* r64 = A.r64 + off;
+  const double* r64 = A.r64 + off64;
   for (int i0 = tid; i0 < nn; i0 += UNR * nthr) {
     // all loads of UNR nodes first, then the updates and stores
     T pv[UNR], qv[UNR], rv[UNR];
@@ -128,10 +136,10 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
     for (int j = 0; j < UNR; ++j) {
       const int i = i0 + j * nthr;
       if (i < nn) {
-        const size_t k = 3 * size_t(i);
-        sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[k];
+        const size_t k = size_t(KS) * i;
+        sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[3 * size_t(i)];
         if (MODE == kSlabUpdate) { pv[j] = pg[k]; qv[j] = qg[k]; rv[j] = r[k]; uv[j] = ug[k]; }
-        else if (MODE == kSlabSync) rv[j] = T(r64[k]);
+        else if (MODE == kSlabSync) rv[j] = T(r64[3 * size_t(i)]);
         else rv[j] = r[k];
       }
     }
@@ -139,7 +147,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
     for (int j = 0; j < UNR; ++j) {
       const int i = i0 + j * nthr;
       if (i < nn) {
-        const size_t k = 3 * size_t(i);
+        const size_t k = size_t(KS) * i;
         const int y = fdiv(i, A.div_n), x = i - y * n;
         T rj = rv[j];
         if (MODE == kSlabUpdate) {
@@ -271,8 +279,8 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
     for (int l = 0; l < A.loads; ++l) any |= A.scal[l].active;
     const int runs = ++A.counters[0];
     A.counters[5] += 1;                                 // loop bodies over the whole solve
-    if (runs >= kMaxBodyRunsSlab) A.counters[1] = 1;  // recorded: loop stopped by the bound
-    cudaGraphSetConditional(A.h, (any && runs < kMaxBodyRunsSlab) ? 1u : 0u);
+    if (runs >= A.cap + 100) A.counters[1] = 1;  // recorded: loop stopped by the bound
+    cudaGraphSetConditional(A.h, (any && runs < A.cap + 100) ? 1u : 0u);
   }
   const LoadScalars& S = A.scal[load];
   if (!S.active) return;
@@ -356,10 +364,14 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
   }
   const T* wv = real_view<T>(res2);
   const size_t node0 = size_t(z) * nn;
-  const size_t off = size_t(load) * 3 * size_t(nn) * n + 3 * node0 + c;
+  constexpr bool PL = sizeof(T) == 4;  // FP32 recurrence vectors are component-planar
+  constexpr int KS = PL ? 1 : 3;
+  const size_t N = size_t(nn) * n;
+  const size_t off = PL ? size_t(load) * 3 * N + size_t(c) * N + node0 : size_t(load) * 3 * N + 3 * node0 + c;
   T* p = reinterpret_cast<T*>(A.p) + off;
-  const double* sc = A.scale + 3 * node0 + c;
-  const float* s32 = sizeof(T) == 4 ? A.scale32 + size_t(c) * nn * n + node0 : nullptr;  // coalesced
+  const size_t dsg = size_t(load / A.lpd) * 3 * size_t(nn) * n;  // this load's design
+  const double* sc = A.scale + dsg + 3 * node0 + c;
+  const float* s32 = sizeof(T) == 4 ? A.scale32 + dsg + size_t(c) * nn * n + node0 : nullptr;  // coalesced
   const T m = T(S.mean_z[c]);
   const T beta = T(S.beta);
   constexpr int UNR = 4;
@@ -370,9 +382,8 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
     for (int j = 0; j < UNR; ++j) {
       const int i = i0 + j * nthr;
       if (i < nn) {
-        const size_t k = 3 * size_t(i);
-        sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[k];
-        pv[j] = A.init ? T(0) : p[k];
+        sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[3 * size_t(i)];
+        pv[j] = A.init ? T(0) : p[size_t(KS) * i];
       }
     }
 #pragma unroll
@@ -382,7 +393,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
         const int y = fdiv(i, A.div_n), x = i - y * n;
         const T w = wv[2 * ((y >> 1) * lpx + x) + (y & 1)];
         const T zv = T(sv[j]) * w - m;
-        p[3 * size_t(i)] = A.init ? zv : zv + beta * pv[j];
+        p[size_t(KS) * i] = A.init ? zv : zv + beta * pv[j];
       }
     }
   }
@@ -453,7 +464,7 @@ static SlabArgs slab_args(pgj_ctx* c, int loads, int prec) {
   A.r64 = c->r64; A.scale = c->scale; A.scale32 = c->scale32; A.spec = c->spec;
   A.tw = prec == PGJ_FP32 ? static_cast<const void*>(static_cast<double2*>(c->tw) + c->n) : c->tw;
   A.scal = c->scal; A.out = c->scal_out; A.partials = c->partials;
-  A.cap = 4000; A.rel_delta2 = c->rel_delta2; A.loads = loads;
+  A.cap = c->cap; A.rel_delta2 = c->rel_delta2; A.loads = loads; A.lpd = c->lpd;
   A.counters = c->cond;
   return A;
 }

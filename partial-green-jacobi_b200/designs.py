@@ -3,6 +3,8 @@
 ``baseline_density``: N(0,1) noise -> periodic Gaussian filter (sigma = n/16 cells) -> smooth
 threshold at the (1 - vf) quantile, rho = logistic((f - q_{1-vf}) / (width * std f)), width 0.1.
 ``simp``: E = Emin + rho^p (E0 - Emin), E0 = 1, p = 3.
+``uneven_designs``: the batched uneven-design workload, one seeded (n, volume fraction, alpha)
+draw per design with n from {24, 32, 48, 64}, vf uniform in [0.2, 0.5] and alpha uniform in [0, 1].
 ``study1_initial`` / ``study1_state0``: the reference's Study I initial design and its state 0,
 material(physical(initial(n, seed), 1)[0]) (exp/asg_topopt_20261103/study.py:61-88).
 """
@@ -28,6 +30,27 @@ def simp(rho: np.ndarray, emin: float, p: float = 3.0) -> np.ndarray:
 
 def baseline_design(n: int, seed: int, emin: float, vf: float = 0.35) -> np.ndarray:
     return simp(baseline_density(n, seed, vf), emin)
+
+
+UNEVEN_GRIDS = (24, 32, 48, 64)
+
+
+def uneven_spec(seed: int) -> tuple[int, float, float]:
+    """(n, volume fraction, alpha) of design `seed` of the uneven batch (its own generator stream)."""
+    rng = np.random.default_rng([seed, 4])
+    n = int(rng.choice(UNEVEN_GRIDS))
+    vf = float(rng.uniform(0.2, 0.5))
+    alpha = float(rng.uniform(0.0, 1.0))
+    return n, vf, alpha
+
+
+def uneven_designs(count: int = 64, emin: float = 1e-6):
+    """Designs 0..count-1 of the uneven batch: [(seed, n, vf, alpha, a)], a = SIMP(baseline density)."""
+    out = []
+    for seed in range(count):
+        n, vf, alpha = uneven_spec(seed)
+        out.append((seed, n, vf, alpha, baseline_design(n, seed, emin, vf)))
+    return out
 
 
 def _study1_physical(x, beta):

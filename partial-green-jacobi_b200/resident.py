@@ -206,6 +206,15 @@ class Operator:
         m = {"reliable": 0, "sweeps": 1}[mode]
         _lib.check(_lib.lib().pgj_set_mixed_mode(self._ctx, m, float(delta)), "pgj_set_mixed_mode")
 
+    def set_iteration_cap(self, cap: int) -> None:
+        """Per-load PCG iteration cap (default 4000, the reference's)."""
+        _lib.check(_lib.lib().pgj_set_iteration_cap(self._ctx, int(cap)), "pgj_set_iteration_cap")
+
+    def set_mixed_operator(self, fp64: bool) -> None:
+        """Mixed contexts: run the recurrence operator in FP64 arithmetic on the FP32 vectors
+        (for weak-material ratios near 1e-9, where FP32 node sums of stiff and weak elements cancel)."""
+        _lib.check(_lib.lib().pgj_set_mixed_operator(self._ctx, 1 if fp64 else 0), "pgj_set_mixed_operator")
+
     def last_refinements(self) -> int:
         return int(_lib.lib().pgj_last_refinements(self._ctx))
 
@@ -301,6 +310,9 @@ class Resident:
         elif method == "compact8":
             # compact law on the density field (exp/asg_gpu_resident_20261103/resident.py:163-168)
             alpha = float(selectors.compact8_alpha(self.op._material_field))
+        elif method == "asg":
+            # frozen ASG MLP on the density field's statistics (resident.py:160-162)
+            alpha = float(selectors.asg_alpha(self.op._material_field))
         else:
             try:
                 alpha = float(method)

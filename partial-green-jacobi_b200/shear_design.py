@@ -68,8 +68,8 @@ def check_args(n: int, steps: int, methods) -> None:
     for m in methods:
         if m not in METHODS:
             raise ValueError(f"unknown method {m!r}; choose from {METHODS}")
-        if m == "asg":
-            raise ValueError("The frozen ASG MLP selector is not provided by this package.")
+        if m == "asg" and (n < 32 or n % 16):
+            raise ValueError("The ASG selector's features need n >= 32 and n a multiple of 16.")
 
 
 def main(argv=None):

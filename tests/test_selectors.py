@@ -73,3 +73,22 @@ def test_selector_resident_choose_on_device(pkg, oracle, golden, method):
               "eta": 13 / 16}[method]
     assert got == pytest.approx(expect, abs=1e-5)
     assert 0.0 < got <= 1.0
+
+
+@pytest.mark.gpu
+def test_resident_select_asg_on_device(pkg, oracle, golden_dir):
+    """Resident.select('asg') on the device density gives the reference network's alpha (the golden
+    prediction of tests/golden/make_asg_golden.py, thresholded at 0.2), and builds that scale."""
+    if not torch.cuda.is_available():  # pragma: no cover - collected on CPU boxes
+        pytest.skip("CUDA device required")
+    g = np.load(golden_dir / "asg_selector.npz")
+    for (n, seed, emin), pred in zip(g["cases"], g["predictions"]):
+        n = int(n)
+        r = pkg.Resident(None, n)
+        a = oracle.simp(oracle.baseline_density(n, int(seed)), float(emin))
+        r.material(torch.tensor(a, device="cuda"))
+        r.select("asg")
+        expect = 0.0 if pred < float(g["threshold"]) else pred
+        assert float(r.alpha) == pytest.approx(expect, abs=2e-5), (n, seed)
+        ref_scale = oracle.scale_field(a, float(r.alpha), *pkg.STUDY1_MEDIUM)
+        assert np.abs(r.op.scale.cpu().numpy() - ref_scale).max() <= 1e-12 * np.abs(ref_scale).max()

@@ -86,6 +86,7 @@ def test_step_limit_and_unstable_objective(pkg):
 def test_argument_checks(pkg, tmp_path):
     sd = pkg.shear_design
     sd.check_args(16, 10, ["0.5", "gj", "green", "compact8", "0.69"])
+    sd.check_args(32, 10, ["asg"])  # the ASG features need n >= 32, a multiple of 16
     for n, steps, methods in ((5, 10, ["0.5"]), (2, 10, ["0.5"]), (16, 0, ["0.5"]), (16, 181, ["0.5"]),
                               (16, 10, ["asg"])):
         with pytest.raises(ValueError):

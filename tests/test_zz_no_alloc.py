@@ -1,7 +1,7 @@
 """The allocation-free C_H entry point gives the same tensor as the context entry point.
 
 pgj_effective_tensor_noalloc exists for callers that cannot allocate device memory (a host that
-owns the whole device pool, or code running under CUDA graph capture). It keeps its scratch in a
+owns the whole device pool and forbids third-party allocations). It keeps its scratch in a
 fixed device array inside the library, so this test calls it through the C ABI twice in a row on
 different inputs (the second call reuses the scratch the first one left behind) and compares each
 result with pgj_effective_tensor run on a regular context. This file is collected last so that a
