@@ -160,6 +160,12 @@ int pgj_set_mixed_mode(pgj_ctx* ctx, int mode, double delta);
  * contrast, and a larger cap lets it certify where the FP64 recurrence needs most of the 4000. */
 int pgj_set_iteration_cap(pgj_ctx* ctx, int cap);
 int pgj_iteration_cap(pgj_ctx* ctx);
+/* Direction update of the FP32 recurrences of a slab-fused PGJ_FP32 context (no reference
+ * counterpart; FP64 contexts keep the reference's beta = r.z / r_prev.z_prev): 1 selects the flexible
+ * (Polak-Ribiere) form beta = r.(z - z_prev) / r_prev.z_prev, which keeps the new direction locally
+ * orthogonal when the FP32 preconditioner apply is inexact; it stores z for the next iteration.
+ * PGJ_ERR_UNSUPPORTED for other contexts. Default 0. */
+int pgj_set_flexible_beta(pgj_ctx* ctx, int on);
 /* Arithmetic of the recurrence operator of a PGJ_FP32 context (no reference counterpart): 0 (default)
  * FP32; 1 FP64 element actions and node sums on the FP32 vectors, for high-contrast designs (weak
  * material ratios near 1e-9), where FP32 node sums of stiff and weak elements cancel. The Green
@@ -193,6 +199,11 @@ int pgj_set_fused_iteration(pgj_ctx* ctx, int on);
  * block, out[1] operator z-planes per block, out[2] rows per x-pass block, out[3] / out[4] kx columns
  * per y / z-pass block, out[5] fused iteration flag. */
 int pgj_tile_shapes(pgj_ctx* ctx, int* out);
+/* The context's tile configuration as the tile table records it (no reference counterpart): out[0..3]
+ * operator rows per block, z-planes per block, plane buffers, occupancy variant; out[4..6] requested FFT
+ * rows per x block, y chunks, z chunks; out[7] fused iteration flag; out[8] where the shapes came from
+ * (0 timed at creation, 1 the tile table built in, 2 environment override). */
+int pgj_tile_config(pgj_ctx* ctx, int* out);
 
 /* Failure-detection self-test (no reference counterpart): runs the bounded device wait used by the
  * kernels' TMA staging on an mbarrier that nothing completes, giving up after `tries` polls.

@@ -141,6 +141,39 @@ def apply_operator(a: np.ndarray, u: np.ndarray, lam: float, mu: float,
     return q
 
 
+_REF_MODAL = None
+
+
+def apply_operator_ref(a: np.ndarray, u: np.ndarray, lam: float, mu: float,
+                       active: np.ndarray | None = None) -> np.ndarray:
+    """q = K(a) u with the reference's own element arithmetic: the exact modal element action of
+    ``solver/src/materials/fi_modal.cuh:2-255`` on C0, times a_e, summed into the nodes
+    (``exp/asg_gpu_resident_20261103/scalar_fi.cu:14-36``). The header is compiled on the host by
+    ``oracle/Makefile`` into ``oracle/_ref/libref_fi_modal.so`` (this container only)."""
+    global _REF_MODAL
+    import ctypes
+    from pathlib import Path
+
+    if _REF_MODAL is None:
+        _REF_MODAL = ctypes.CDLL(str(Path(__file__).resolve().parent / "_ref" / "libref_fi_modal.so"))
+        _REF_MODAL.ref_fi_modal_batch.restype = None
+    n = a.shape[0]
+    u = np.atleast_2d(u)
+    ue = np.ascontiguousarray(_gather(_as_nodes(u, n)))
+    fe = np.empty_like(ue)
+    c21 = np.ascontiguousarray(packed21(lam, mu))
+    h = 1.0 / n
+    g = np.array([1 / (4 * h)] * 3 + [h ** 3])
+    vp = ctypes.c_void_p
+    _REF_MODAL.ref_fi_modal_batch(vp(ue.ctypes.data), vp(c21.ctypes.data), vp(g.ctypes.data), vp(fe.ctypes.data),
+                                  ctypes.c_long(ue.shape[0] * ue.shape[1]))
+    fe *= a.reshape(1, -1, 1)
+    q = _scatter(fe, n)
+    if active is not None:
+        q[~np.asarray(active, bool)] = 0.0
+    return q
+
+
 def rhs(a: np.ndarray, macro: np.ndarray, lam: float, mu: float) -> np.ndarray:
     """Periodic nodal forces f = -V sum_{8 el} B_c^T (a_e C0) eps (``hybrid_kernels.cu:50-68``)."""
     n = a.shape[0]
@@ -299,8 +332,11 @@ class Problem:
         return self.a.shape[0]
 
     reverse: bool = False
+    ref_arith: bool = False
 
     def K(self, u, active=None):
+        if self.ref_arith:
+            return apply_operator_ref(self.a, u, self.lam, self.mu, active)
         return apply_operator(self.a, u, self.lam, self.mu, active, self.reverse)
 
     def B(self, r):
@@ -325,6 +361,8 @@ def solve_batch(prob: Problem, f: np.ndarray, u0: np.ndarray | None = None, rtol
     ``order`` "b" runs the same recurrence with the recurrence dot products and the operator's
     corner sums in another order: equal in exact arithmetic, rounded differently. An iteration
     count that agrees between the two orders is stable against rounding-level perturbations.
+    ``order`` "r" evaluates the operator with the reference's own modal element arithmetic
+    (``apply_operator_ref``) instead of the dense 24 x 24 element product.
 
     ``max_iterations`` bounds the total PCG iterations run (timing samples only); a bounded run
     returns whatever state it reached.
@@ -333,8 +371,9 @@ def solve_batch(prob: Problem, f: np.ndarray, u0: np.ndarray | None = None, rtol
     """
     L = f.shape[0]
     n = prob.n
-    dot = {"a": _dot_a, "b": _dot_b}[order]
+    dot = {"a": _dot_a, "b": _dot_b, "r": _dot_a}[order]
     prob.reverse = order == "b"
+    prob.ref_arith = order == "r"
     u = np.zeros_like(f) if u0 is None else np.array(u0, dtype=np.float64)
     norm = np.sqrt((f * f).sum(1))
     target2 = np.maximum(norm * rtol, np.full_like(norm, 1e-13 / math.sqrt(n))) ** 2

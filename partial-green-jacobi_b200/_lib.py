@@ -71,12 +71,14 @@ SIGNATURES = {
     "pgj_set_mixed_mode": (C.c_int, [vp, C.c_int, f64]),
     "pgj_set_mixed_operator": (C.c_int, [vp, C.c_int]),
     "pgj_set_iteration_cap": (C.c_int, [vp, C.c_int]),
+    "pgj_set_flexible_beta": (C.c_int, [vp, C.c_int]),
     "pgj_iteration_cap": (C.c_int, [vp]),
     "pgj_last_refinements": (C.c_int, [vp]),
     "pgj_last_launches": (C.c_longlong, [vp]),
     "pgj_selftest_wait_timeout": (C.c_int, [vp, C.c_int, vp]),
     "pgj_fused_iteration": (C.c_int, [vp]),
     "pgj_tile_shapes": (C.c_int, [vp, C.POINTER(C.c_int)]),
+    "pgj_tile_config": (C.c_int, [vp, C.POINTER(C.c_int)]),
     "pgj_set_fused_iteration": (C.c_int, [vp, C.c_int]),
     "pgj_profile_iteration": (C.c_int, [vp, C.c_int, vp, C.c_int, vp, vp, vp]),
     "pgj_energies": (C.c_int, [vp, C.c_int, vp, vp, vp, vp]),

@@ -33,7 +33,8 @@ def needs_build() -> bool:
     if not OUT.exists():
         return True
     stamp = OUT.stat().st_mtime
-    deps = list(sources()) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + [HERE.parent / "include/pgj.h"]
+    deps = (list(sources()) + list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.inc"))
+            + [HERE.parent / "include/pgj.h"])
     return any(p.stat().st_mtime > stamp for p in deps)
 
 

@@ -168,6 +168,7 @@ struct LoadScalars {
   int total_iterations;  // mixed refinement: inner iterations summed over sweeps
   int frozen;       // batched contexts: this load's design took its last attempt (later attempts skip it)
   int restarts;     // restarts taken by this load's design
+  double rz_cross;  // flexible beta: new residual . previous preconditioned residual
   int ticket[8];    // per-kernel block tickets for the last-block finalizers
 };
 

@@ -76,7 +76,7 @@ static Layout make_layout(int n, int D, int lpd, int prec) {
   y.aux = take(sizeof(double) * kAuxDoubles);
   // twiddles (double2[n], float2[n]) and the per-axis Green factors (float4[n]: m, v, d)
   y.tw = take(size_t(n) * (sizeof(double2) + sizeof(float2) + sizeof(float4)));
-  const size_t pslots = size_t(4 * L > 24 ? 4 * L : 24);
+  const size_t pslots = size_t(kPartialQ * L > 24 ? kPartialQ * L : 24);
   y.partials = take(sizeof(double) * pslots * kMaxPartials);
   y.a = take(sizeof(double) * N * D);
   y.scale = take(sizeof(double) * N3 * D);
@@ -598,6 +598,15 @@ int pgj_set_iteration_cap(pgj_ctx* c, int cap) {
 
 int pgj_iteration_cap(pgj_ctx* c) { return c ? c->cap : -1; }
 
+int pgj_set_flexible_beta(pgj_ctx* c, int on) {
+  if (!c || (on != 0 && on != 1)) return PGJ_ERR_ARGUMENT;
+  if (on && !(c->prec == PGJ_FP32 && c->fused)) return PGJ_ERR_UNSUPPORTED;
+  c->flex = on;
+  c->graphs->loads = 0;  // a parameter of the captured kernels
+  c->graphs->attempt_loads = 0;
+  return PGJ_OK;
+}
+
 int pgj_set_mixed_operator(pgj_ctx* c, int fp64) {
   if (!c || (fp64 != 0 && fp64 != 1)) return PGJ_ERR_ARGUMENT;
   if (c->prec != PGJ_FP32) return fp64 ? PGJ_OK : PGJ_ERR_UNSUPPORTED;  // FP64 contexts are FP64 throughout
@@ -786,6 +795,14 @@ int pgj_tile_shapes(pgj_ctx* c, int* out) {
   if (!c || !out) return PGJ_ERR_ARGUMENT;
   out[0] = c->sg.ty; out[1] = c->sg.zc; out[2] = c->fg.rb; out[3] = c->fg.kcy; out[4] = c->fg.kcz;
   out[5] = c->fused;
+  return PGJ_OK;
+}
+
+int pgj_tile_config(pgj_ctx* c, int* out) {
+  if (!c || !out) return PGJ_ERR_ARGUMENT;
+  out[0] = c->sg.ty; out[1] = c->sg.zc; out[2] = c->sg.stages; out[3] = c->sg.occ;
+  out[4] = c->fft_req[0]; out[5] = c->fft_req[1]; out[6] = c->fft_req[2];
+  out[7] = c->fused; out[8] = c->tile_source;
   return PGJ_OK;
 }
 

@@ -18,6 +18,8 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <utility>
+#include <array>
 #include <tuple>
 #include <vector>
 
@@ -116,6 +118,7 @@ struct GreenArgs {
   int forward_only;      // FZ: forward transform along z only (builds shat)
   int unit_input;        // FX: transform s itself (r ignored; builds shat)
   const float4* axis;    // per-axis symbol factors (m, v, d), FP32 z pass at n = 64
+  int flex;              // flexible beta: beta = (rz_new - r_new . z_prev) / rz
   double lam, mu;
 };
 
@@ -312,7 +315,7 @@ __global__ void __launch_bounds__(512) k_fz(const GreenArgs A) {
         S.beta = 0.0;
       } else {
         const double rz = S.rz;
-        S.beta = rzn / (rz != 0.0 ? rz : 1.0);
+        S.beta = (A.flex ? rzn - S.rz_cross : rzn) / (rz != 0.0 ? rz : 1.0);
       }
       S.rz = rzn;
       if (A.fused)
@@ -492,7 +495,7 @@ __global__ void __launch_bounds__(WPB * 32, MINB) k_fz64(const GreenArgs A) {
         S.beta = 0.0;
       } else {
         const double rz = S.rz;
-        S.beta = rzn / (rz != 0.0 ? rz : 1.0);
+        S.beta = (A.flex ? rzn - S.rz_cross : rzn) / (rz != 0.0 ? rz : 1.0);
       }
       S.rz = rzn;
       for (int k = 0; k < 3; ++k) S.mean_z[k] = mz[k] / double(size_t(N) * N * N);
@@ -691,6 +694,7 @@ int launch_fz_fused(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s) 
   A.finalize_fz = 1;
   A.fused = 1;
   A.shat = c->shat;
+  A.flex = prec == PGJ_FP32 ? c->flex : 0;
   const char* e = std::getenv("PGJ_FZ64");
   if (c->n == 64 && !(e && e[0] == '0'))  // line transforms in registers (PGJ_FZ64=0: generic pass)
     return prec == PGJ_FP32 ? run_fz64<float>(c, loads, A, s) : run_fz64<double>(c, loads, A, s);
@@ -741,18 +745,31 @@ int launch_green_standalone(pgj_ctx* c, int loads, const double* r, double* z, c
 // tile shapes (rows per x block, y-chunks, z-chunks) on the context's buffers; cached per (n, loads
 // per design, precision), so batched contexts share the choice with single ones.
 static std::mutex g_fft_mutex;
-static std::map<std::tuple<int, int, int>, FFTGeom> g_fft_tuned;
+static std::map<std::tuple<int, int, int>, std::pair<FFTGeom, std::array<int, 3>>> g_fft_tuned;
 
 int autotune_fft(pgj_ctx* c, cudaStream_t s) {
   const auto key = std::make_tuple(c->n, c->lpd, c->prec);
   {
     std::lock_guard<std::mutex> lock(g_fft_mutex);
     auto it = g_fft_tuned.find(key);
-    if (it != g_fft_tuned.end()) { c->fg = it->second; return PGJ_OK; }
+    if (it != g_fft_tuned.end()) {
+      c->fg = it->second.first;
+      for (int k = 0; k < 3; ++k) c->fft_req[k] = it->second.second[k];
+      return PGJ_OK;
+    }
   }
   if (std::getenv("PGJ_FFT_RB") || std::getenv("PGJ_FFT_NKY") || std::getenv("PGJ_FFT_NKZ")) return PGJ_OK;
   const int eb = c->prec == PGJ_FP32 ? 4 : 8;
+  TileEntry t;
+  if (tile_table(c->n, c->prec, &t)) {
+    c->fg = fft_geom(c->n, eb, c->plan, t.rb, t.nky, t.nkz);
+    c->fft_req[0] = t.rb; c->fft_req[1] = t.nky; c->fft_req[2] = t.nkz;
+    std::lock_guard<std::mutex> lock(g_fft_mutex);
+    g_fft_tuned[key] = {c->fg, {t.rb, t.nky, t.nkz}};
+    return PGJ_OK;
+  }
   std::vector<FFTGeom> cands;
+  std::vector<std::array<int, 3>> reqs;
   for (int rb : {8, 16})
     for (int nky : {1, 2, 3})
       for (int nkz : {1, 2, 3, 4, 6}) {
@@ -760,7 +777,7 @@ int autotune_fft(pgj_ctx* c, cudaStream_t s) {
         bool dup = false;
         for (const FFTGeom& h : cands)
           dup = dup || (h.rb == g.rb && h.kcy == g.kcy && h.kcz == g.kcz);
-        if (!dup) cands.push_back(g);
+        if (!dup) { cands.push_back(g); reqs.push_back({rb, nky, nkz}); }
       }
   GreenArgs A = green_args(c, c->prec, c->r);
   A.skip_inactive = 0;
@@ -770,10 +787,12 @@ int autotune_fft(pgj_ctx* c, cudaStream_t s) {
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   FFTGeom best = c->fg;
+  std::array<int, 3> best_req = {0, 0, 0};
   float best_ms = 1e30f;
   for (int r = 0; r < 10; ++r)  // bring the clocks up before timing anything
     c->prec == PGJ_FP32 ? run_green<float>(c, c->lpd, A, s) : run_green<double>(c, c->lpd, A, s);
-  for (const FFTGeom& g : cands) {
+  for (size_t ci = 0; ci < cands.size(); ++ci) {
+    const FFTGeom& g = cands[ci];
     c->fg = g;
     A.geo = g;
     int st = c->prec == PGJ_FP32 ? run_green<float>(c, c->lpd, A, s) : run_green<double>(c, c->lpd, A, s);
@@ -789,13 +808,14 @@ int autotune_fft(pgj_ctx* c, cudaStream_t s) {
       cudaEventElapsedTime(&t, e0, e1);
       ms = t < ms ? t : ms;
     }
-    if (ms < best_ms) { best_ms = ms; best = g; }
+    if (ms < best_ms) { best_ms = ms; best = g; best_req = reqs[ci]; }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   c->fg = best;
+  c->fft_req[0] = best_req[0]; c->fft_req[1] = best_req[1]; c->fft_req[2] = best_req[2];
   std::lock_guard<std::mutex> lock(g_fft_mutex);
-  g_fft_tuned[key] = best;
+  g_fft_tuned[key] = {best, best_req};
   return check_launch();
 }
 

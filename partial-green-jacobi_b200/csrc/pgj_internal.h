@@ -63,7 +63,7 @@ struct StencilArgs {
 
 // Partial-sum slots per load per kernel (blocks per load upper bound).
 constexpr int kMaxPartials = 4096;
-constexpr int kPartialQ = 4;
+constexpr int kPartialQ = 5;
 // aux block: [0,24) stiffness diagonal per local node, [32,68) unit Voigt macros,
 // [128, 128 + kMaxPartials) scalar-reduction partials of the scale build.
 constexpr int kAuxVoigt = 32;
@@ -125,6 +125,9 @@ struct pgj_ctx {
   int mixed_mode;      // 0 reliable-update CG, 1 restarted refinement sweeps
   int op64;            // FP32 contexts: the recurrence operator computes in FP64 (FP32 vectors)
   int cap;             // per-load PCG iteration cap (4000, the reference's, unless set)
+  int flex;            // FP32 slab-fused recurrences: flexible (Polak-Ribiere) beta
+  int tile_source;     // 0 tuned by timing at creation, 1 tile table, 2 environment override
+  int fft_req[3];      // requested FFT tiles (rows per x block, y chunks, z chunks)
   int last_refinements;
   int pending_loads;       // loads of the solve enqueued by pgj_solve_async
   int diag_staged;         // stiffness-diagonal constants copied to aux
@@ -137,8 +140,13 @@ struct pgj_ctx {
 
 namespace pgj {
 // operator (pgj_operator.cu)
+// planar_plain: plain mode on the component-planar FP32 layout of a slab-fused context (the tuner)
 int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, void* out, const double* f,
-                   const int32_t* active_ext, cudaStream_t s, const LoadScalars* rel_flags = nullptr);
+                   const int32_t* active_ext, cudaStream_t s, const LoadScalars* rel_flags = nullptr,
+                   bool planar_plain = false);
+// offline-tuned tile shapes per (n, precision)
+struct TileEntry { int n, prec, ty, zc, stages, occ, rb, nky, nkz; };
+bool tile_table(int n, int prec, TileEntry* out);
 int launch_rhs(pgj_ctx* c, int loads, const double* macros_dev, double* f, cudaStream_t s);
 int launch_scale(pgj_ctx* c, double alpha, cudaStream_t s);
 int launch_project_u(pgj_ctx* c, int loads, double* u, cudaStream_t s);

@@ -257,8 +257,9 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   if (!act) {
     if (MODE == kPlain && out_row) {
       for (int z = z0; z < z0 + zc; ++z) {
-        T* o = out + 3 * ((size_t(z) * n + ey) * n + tx);
-        o[0] = T(0); o[1] = T(0); o[2] = T(0);
+        const size_t node = (size_t(z) * n + ey) * n + tx;
+        T* o = out + (PL ? node : 3 * node);
+        o[0] = T(0); o[PL ? N : 1] = T(0); o[PL ? 2 * N : 2] = T(0);
       }
     }
     return;
@@ -615,6 +616,25 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   }
 }
 
+// Tile table: shapes per (grid edge, precision) picked offline by the project's tuner
+// (partial-green-jacobi_b200/tune_tiles.py, which times every candidate on a B200 and writes
+// pgj_tiles.inc). Contexts of a tabulated size take these shapes without timing anything, so the
+// block decomposition, and with it the summation order of every block-partial reduction, is the
+// same in every process, batch size and run. Sizes outside the table are tuned by timing at
+// context creation (below); PGJ_AUTOTUNE=1 forces timing for every size (that is how the table is
+// made).
+static const TileEntry kTileTable[] = {
+#include "pgj_tiles.inc"
+    {0, 0, 0, 0, 0, 0, 0, 0, 0}};
+
+bool tile_table(int n, int prec, TileEntry* out) {
+  if (const char* e = std::getenv("PGJ_AUTOTUNE"))
+    if (e[0] == '1') return false;
+  for (const TileEntry& t : kTileTable)
+    if (t.n == n && t.prec == prec) { *out = t; return true; }
+  return false;
+}
+
 // Tile autotuner: times the operator (the loads of one design, plain mode) for candidate tile shapes
 // on the context's own buffers and keeps the fastest. Results are cached per (n, loads per design,
 // precision) for the process, so contexts created later, batched ones included, reuse the choice
@@ -628,10 +648,26 @@ int autotune_stencil(pgj_ctx* c, cudaStream_t s) {
   {
     std::lock_guard<std::mutex> lock(g_tune_mutex);
     auto it = g_tuned.find(key);
-    if (it != g_tuned.end()) { c->sg = it->second; return PGJ_OK; }
+    if (it != g_tuned.end()) {
+      c->sg = it->second;
+      TileEntry t;
+      c->tile_source = tile_table(n, c->prec, &t) ? 1 : 0;
+      return PGJ_OK;
+    }
   }
-  if (std::getenv("PGJ_STENCIL_TY") || std::getenv("PGJ_STENCIL_ZC") || std::getenv("PGJ_STENCIL_OCC"))
+  if (std::getenv("PGJ_STENCIL_TY") || std::getenv("PGJ_STENCIL_ZC") || std::getenv("PGJ_STENCIL_OCC")) {
+    c->tile_source = 2;
     return PGJ_OK;  // manual override
+  }
+  TileEntry t;
+  if (tile_table(n, c->prec, &t)) {
+    c->sg = stencil_geom_shape(n, t.ty, t.zc, t.stages, t.occ);
+    c->tile_source = 1;
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tuned[key] = c->sg;
+    return PGJ_OK;
+  }
+  c->tile_source = 0;
   std::vector<int> tys;
   for (int ty : {1, 2, 3, 4, 5, 6, 7, 8, 12, 16, 31})
     if (ty <= n && n * (ty + 1) <= 512 && (ty + 1) * n >= 32) tys.push_back(ty);
@@ -647,7 +683,7 @@ int autotune_stencil(pgj_ctx* c, cudaStream_t s) {
   const void* in = c->p;
   void* out = c->q;
   // bring the clocks up before timing anything
-  for (int r = 0; r < 30; ++r) launch_stencil(c, kPlain, c->lpd, c->prec, in, out, nullptr, nullptr, s);
+  for (int r = 0; r < 30; ++r) launch_stencil(c, kPlain, c->lpd, c->prec, in, out, nullptr, nullptr, s, nullptr, true);
   for (int ty : tys)
     for (int zc : zcs)
       for (int occ : {1, 3})
@@ -656,12 +692,12 @@ int autotune_stencil(pgj_ctx* c, cudaStream_t s) {
         StencilGeom g = stencil_geom_shape(n, ty, zc, stages, occ);
         if (g.ntiles * g.nchunks > kMaxPartials) continue;
         c->sg = g;
-        int st = launch_stencil(c, kPlain, c->lpd, c->prec, in, out, nullptr, nullptr, s);  // warm
+        int st = launch_stencil(c, kPlain, c->lpd, c->prec, in, out, nullptr, nullptr, s, nullptr, true);  // warm
         if (st) { cudaEventDestroy(e0); cudaEventDestroy(e1); return st; }
         float ms = 1e30f;
         for (int trial = 0; trial < 2; ++trial) {  // best of two trials of five launches
           cudaEventRecord(e0, s);
-          for (int r = 0; r < 5; ++r) launch_stencil(c, kPlain, c->lpd, c->prec, in, out, nullptr, nullptr, s);
+          for (int r = 0; r < 5; ++r) launch_stencil(c, kPlain, c->lpd, c->prec, in, out, nullptr, nullptr, s, nullptr, true);
           cudaEventRecord(e1, s);
           cudaEventSynchronize(e1);
           float t = 0.f;
@@ -706,6 +742,7 @@ static void set_stencil_smem(int lim) {
   cudaFuncSetAttribute(k_stencil<double, kResidual, OCC>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_stencil<float, kPCG, OCC, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_stencil<float, kPCG, OCC, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_stencil<float, kPlain, OCC, float, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_stencil<float, kPCG, OCC, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 
@@ -719,7 +756,8 @@ template <int OCC>
 static void launch_stencil_kernel(int mode, int prec, bool r64, bool planar, dim3 grid, dim3 block, size_t smem,
                                   cudaStream_t s, const StencilArgs& A) {
   if (prec == PGJ_FP32) {
-    if (mode == kPlain) k_stencil<float, kPlain, OCC><<<grid, block, smem, s>>>(A);
+    if (mode == kPlain && planar) k_stencil<float, kPlain, OCC, float, true><<<grid, block, smem, s>>>(A);
+    else if (mode == kPlain) k_stencil<float, kPlain, OCC><<<grid, block, smem, s>>>(A);
     else if (planar && r64) k_stencil<float, kPCG, OCC, double, true><<<grid, block, smem, s>>>(A);
     else if (planar) k_stencil<float, kPCG, OCC, float, true><<<grid, block, smem, s>>>(A);
     else if (r64) k_stencil<float, kPCG, OCC, double><<<grid, block, smem, s>>>(A);
@@ -732,7 +770,7 @@ static void launch_stencil_kernel(int mode, int prec, bool r64, bool planar, dim
 }
 
 int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, void* out, const double* f,
-                   const int32_t* active_ext, cudaStream_t s, const LoadScalars* rel_flags) {
+                   const int32_t* active_ext, cudaStream_t s, const LoadScalars* rel_flags, bool planar_plain) {
   const int n = c->n;
   StencilArgs A;
   A.n = n; A.ty = c->sg.ty; A.zc = c->sg.zc;
@@ -743,7 +781,7 @@ int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, vo
   A.rel_flags = rel_flags;
   const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
   // the FP32 recurrence vectors of a slab-fused context are component-planar, (3, N) per load
-  const bool planar = prec == PGJ_FP32 && mode == kPCG && c->fused;
+  const bool planar = prec == PGJ_FP32 && c->fused && (mode == kPCG || (mode == kPlain && planar_plain));
   // TMA rows need 16-byte aligned starts and sizes: (3 n * element size) % 16 == 0 and an aligned base
   // (component-planar rows: n * element size, the component blocks 4 n^3 bytes apart)
   const size_t rowb = (planar ? 1 : 3) * size_t(n) * tsz;

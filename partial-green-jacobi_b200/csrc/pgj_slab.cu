@@ -36,6 +36,8 @@ struct SlabArgs {
   const double* scale;    // (designs, 3N) FP64 scale field s
   const float* scale32;   // FP32 contexts: (designs, 3, N) component-planar FP32 copy of s
   void* spec;             // (L,3,n,n,nsp) complex T
+  void* zprev;            // flexible beta: (L,3N) T preconditioned residual of the previous direction
+  int flex;               // flexible beta: fxy sums r_new . z_prev, ifxy stores z
   const void* tw;         // n complex T twiddles
   LoadScalars* scal;      // recurrence records
   const LoadScalars* out; // sync mode: certificate records (res2, mean r of the true residual)
@@ -118,13 +120,14 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   const float* s32 = sizeof(T) == 4 ? A.scale32 + dsg * N3 + size_t(c) * nn * n + node0 : nullptr;  // coalesced
   T* packed = real_view<T>(b0);
   const int lpx = R64 ? kLine64 : n + 1;  // pitch of the packed x lines
-  double acc[2] = {0.0, 0.0};
+  double acc[3] = {0.0, 0.0, 0.0};
   const double alpha = MODE == kSlabUpdate ? S.alpha : 0.0;
   const T a = T(alpha);
   // nodes whose loads are in flight together (the FP64 update keeps five doubles per node)
   constexpr int UNR = (MODE == kSlabUpdate && sizeof(T) == 8) ? 2 : 4;
   const T* pg = reinterpret_cast<const T*>(A.p) + off;
   const T* qg = reinterpret_cast<const T*>(A.q) + off;
+  const T* zg = A.flex ? reinterpret_cast<const T*>(A.zprev) + off : nullptr;
   U* ug = reinterpret_cast<U*>(A.u) + off;
   const double* r64 = A.r64 + off64;
   for (int i0 = tid; i0 < nn; i0 += UNR * nthr) {
@@ -157,6 +160,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
           const double rd = double(rj);
           acc[0] += rd * rd;
           acc[1] += rd;
+          if (zg) acc[2] += rd * double(zg[k]);
         } else if (MODE == kSlabSync) {
           r[k] = rj;
         }
@@ -227,16 +231,18 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   const int nblk = 3 * n, blk = c + 3 * z;
   double* part = A.partials + size_t(load) * kPartialQ * kMaxPartials;
   if (MODE == kSlabUpdate) {
-    block_sum<2>(acc, red);
+    block_sum<3>(acc, red);
     if (tid == 0) {
       part[blk] = acc[0];
       for (int cc = 0; cc < 3; ++cc) part[(1 + cc) * kMaxPartials + blk] = cc == c ? acc[1] : 0.0;
+      part[4 * kMaxPartials + blk] = acc[2];
     }
     if (!last_block(&S.ticket[kTicketUpdate], nblk)) return;
     if (tid < 32) {
-      double v[4];
-      for (int k = 0; k < 4; ++k) v[k] = warp_sum_partials(part + k * kMaxPartials, nblk);
+      double v[5];
+      for (int k = 0; k < 5; ++k) v[k] = warp_sum_partials(part + k * kMaxPartials, nblk);
       if (tid == 0) {
+        S.rz_cross = v[4];
         // same bookkeeping as the unfused update (k_update_ur)
         const double res2 = v[0];
         const bool finite = isfinite(res2);
@@ -394,15 +400,16 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
         const T w = wv[2 * ((y >> 1) * lpx + x) + (y & 1)];
         const T zv = T(sv[j]) * w - m;
         p[size_t(KS) * i] = A.init ? zv : zv + beta * pv[j];
+        if (A.flex) reinterpret_cast<T*>(A.zprev)[off + size_t(KS) * i] = zv;
       }
     }
   }
 }
 
 // ------------------------------------------------------------------------------------ host side
-static size_t slab_smem(int n, int nsp, size_t tsz) { return 2 * size_t(n) * nsp * 2 * tsz + 32 * 2 * 8 + 64; }
+static size_t slab_smem(int n, int nsp, size_t tsz) { return 2 * size_t(n) * nsp * 2 * tsz + 32 * 3 * 8 + 64; }
 // R64: 36 lines of kLine64 complex values, then the n x nsp rows, then the reduction
-static size_t slab_smem64(int nsp, size_t tsz) { return (36 * size_t(kLine64) + 64 * size_t(nsp)) * 2 * tsz + 32 * 2 * 8 + 64; }
+static size_t slab_smem64(int nsp, size_t tsz) { return (36 * size_t(kLine64) + 64 * size_t(nsp)) * 2 * tsz + 32 * 3 * 8 + 64; }
 
 static int slab_threads(const pgj_ctx* c) {
   int minr = 8;
@@ -462,6 +469,8 @@ static SlabArgs slab_args(pgj_ctx* c, int loads, int prec) {
   A.div_nh = make_fastdiv(unsigned(c->n / 2));
   A.p = c->p; A.q = c->q; A.r = c->r;
   A.r64 = c->r64; A.scale = c->scale; A.scale32 = c->scale32; A.spec = c->spec;
+  A.flex = prec == PGJ_FP32 ? c->flex : 0;
+  A.zprev = c->sw;  // unused by the fused form otherwise
   A.tw = prec == PGJ_FP32 ? static_cast<const void*>(static_cast<double2*>(c->tw) + c->n) : c->tw;
   A.scal = c->scal; A.out = c->scal_out; A.partials = c->partials;
   A.cap = c->cap; A.rel_delta2 = c->rel_delta2; A.loads = loads; A.lpd = c->lpd;

@@ -210,6 +210,10 @@ class Operator:
         """Per-load PCG iteration cap (default 4000, the reference's)."""
         _lib.check(_lib.lib().pgj_set_iteration_cap(self._ctx, int(cap)), "pgj_set_iteration_cap")
 
+    def set_flexible_beta(self, on: bool) -> None:
+        """Mixed contexts: Polak-Ribiere direction updates of the FP32 recurrences."""
+        _lib.check(_lib.lib().pgj_set_flexible_beta(self._ctx, 1 if on else 0), "pgj_set_flexible_beta")
+
     def set_mixed_operator(self, fp64: bool) -> None:
         """Mixed contexts: run the recurrence operator in FP64 arithmetic on the FP32 vectors
         (for weak-material ratios near 1e-9, where FP32 node sums of stiff and weak elements cancel)."""

@@ -20,11 +20,13 @@ solver). Every step is issued asynchronously; the loop polls CUDA events and nev
 request while others could be admitted. Results are identical whether a request runs alone or in a
 mix: each context is private to one request at a time and every kernel reduces in a fixed order.
 
-Precision. A mixed server runs FP32 inner recurrences (FP64 certificate) where they pay: lineages
-whose Emin is below ``fp64_below_emin`` (a contrast the FP32 operator no longer resolves, so the
-FP32 recurrence stalls near the target) run in FP64 from the start, and any mixed request that fails
-certification is redone in FP64, warm-started from the mixed iterate. A design step commits its OC
-update only once its solve is certified.
+Precision. A mixed server runs FP32 inner recurrences (FP64 certificate); any mixed request that
+fails certification is redone in FP64, warm-started from the mixed iterate, and lineages whose Emin is
+below ``fp64_below_emin`` (default 0: none) run in FP64 from the start. A lineage without a fixed alpha
+takes the eta-lookup exponent of its weak-material ratio (9/16, 11/16, 13/16 for Emin 1e-4, 1e-6,
+1e-9; the reference's replay study, exp/asg_density_selector_20261105/run.py:57), with which the
+mixed recurrence certifies up to Emin 1e-9. A design step commits its OC update only once its solve
+is certified.
 """
 from __future__ import annotations
 
@@ -38,13 +40,18 @@ import numpy as np
 from . import _lib
 from .designs import baseline_density
 from .outer import PaperOuter
-from .resident import PAPER_MEDIUM, Operator
+from .resident import ETA_ANCHORS, PAPER_MEDIUM, Operator
 
 
 def _torch():
     import torch
 
     return torch
+
+
+def eta_alpha(emin: float) -> float:
+    """Eta-lookup exponent of the nearest calibrated weak-material ratio (log scale)."""
+    return ETA_ANCHORS[min(ETA_ANCHORS, key=lambda k: abs(math.log10(k) - math.log10(emin)))]
 
 
 def supported_n(n: int) -> bool:
@@ -81,7 +88,7 @@ class Lineage:
     emin: float = 1e-6
     steps: int = 30
     volume: float = 0.3
-    alpha: float = 0.5
+    alpha: float | None = None  # None: the eta lookup of emin
     rmin: float = 1.5
     move: float = 0.2
     beta: float = 4.0
@@ -177,7 +184,7 @@ class Server:
     """Continuous batching over libpgj contexts under an HBM budget (bytes)."""
 
     def __init__(self, precision: str = "mixed", hbm_budget: float = 120e9, max_workers_per_n: int = 4,
-                 rtol: float = 1e-8, medium=PAPER_MEDIUM, fp64_below_emin: float = 1e-7, fallback: bool = True):
+                 rtol: float = 1e-8, medium=PAPER_MEDIUM, fp64_below_emin: float = 0.0, fallback: bool = True):
         self.precision = precision
         self.fp64_below_emin = float(fp64_below_emin)
         self.fallback = bool(fallback)
@@ -274,7 +281,7 @@ class Server:
                     ls.pending_advance = False
                 ls.outer.evaluate()                     # filter + projection + SIMP -> outer.a
                 w.op.set_material(ls.outer.a)
-                w.op.set_alpha(job.req.alpha)
+                w.op.set_alpha(job.req.alpha if job.req.alpha is not None else eta_alpha(job.req.emin))
                 u = ls.u                                # warm start, updated in place
             else:
                 a = torch.as_tensor(job.req.a, dtype=torch.float64)

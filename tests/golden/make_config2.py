@@ -6,8 +6,10 @@ Each case is one certified six-load homogenization of a seeded synthetic design 
 periodic Gaussian sigma = n/16, logistic threshold to volume fraction 0.35, SIMP p = 3 with
 E0 = 1, nu = 0.3), zero start, relative true residual 1e-8, solved by the oracle twice: in its
 default summation order ("a") and in a second order ("b": recurrence dots and operator corner
-sums reordered). The fixture keeps C_H, the per-load iteration counts of both orders, the
-relative true residuals and the rhs norms. An iteration count that is equal in both orders is
+sums reordered), and for some cases a third time with the operator evaluated by the reference's own
+modal element arithmetic ("r", fi_modal.cuh compiled on the host by oracle/Makefile). The fixture
+keeps C_H, the per-load iteration counts of every order, the relative true residuals and the rhs
+norms. An iteration count that is equal in both orders is
 "stable": the GPU tests assert it exactly; the others get the stated tolerance.
 
 Grids: n = 32, alpha in {0, 0.5, 1} x Emin/E0 in {1e-4, 1e-6, 1e-9} x seeds 0..4 (45 cases),
@@ -86,10 +88,12 @@ def merge(records: list[dict]) -> dict:
             continue
         a = d["a"]
         b = d.get("b")
+        r = d.get("r")
         out[k] = dict(n=a["n"], alpha=a["alpha"], emin=a["emin"], seed=a["seed"], C=a["C"],
                       iterations=a["iterations"],
                       iterations_b=b["iterations"] if b else None,
                       C_b=b["C"] if b else None,
+                      iterations_r=r["iterations"] if r else None,
                       relative_residual=a["relative_residual"], rhs_norm=a["rhs_norm"],
                       converged=a["converged"], restarts=a["restarts"], raised=a["raised"])
     return out
@@ -102,6 +106,8 @@ def main():
     ap.add_argument("--checkpoint", default="/tmp/pgj_config2_checkpoint.jsonl")
     ap.add_argument("--out", default=str(HERE / "config2.json"))
     ap.add_argument("--merge-only", action="store_true", help="write the fixture from the checkpoint, run nothing")
+    ap.add_argument("--orders", default="ab", help="a: default, b: reordered sums, r: the reference's modal "
+                                                   "element arithmetic (needs oracle/_ref, built by oracle/Makefile)")
     args = ap.parse_args()
 
     ckpt = Path(args.checkpoint)
@@ -109,7 +115,7 @@ def main():
     if ckpt.exists():
         done = [json.loads(line) for line in ckpt.read_text().splitlines() if line.strip()]
     have = {(r["key"], r["order"]) for r in done}
-    todo = [(c, o) for c in cases(args.set) for o in ("a", "b") if (key(c), o) not in have]
+    todo = [(c, o) for c in cases(args.set) for o in args.orders if (key(c), o) not in have]
     print(f"{len(done)} runs checkpointed, {len(todo)} to go", flush=True)
 
     import multiprocessing as mp

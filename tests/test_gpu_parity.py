@@ -547,7 +547,7 @@ def test_serving_design_step_matches_oracle_chain(pkg, oracle):
     update against the CPU restatement."""
     sv = pkg.serve
     n = 10
-    lin = sv.Lineage(n=n, seed=4, emin=1e-4, steps=1, volume=0.3, rmin=1.5, move=0.2, tag=0)
+    lin = sv.Lineage(n=n, seed=4, emin=1e-4, steps=1, volume=0.3, alpha=0.5, rmin=1.5, move=0.2, tag=0)
     res = sv.Server(precision="fp64").run([sv.Arrival(0.0, lin)], realtime=False)
     assert len(res) == 1 and res[0].status == 0
     lam, mu = pkg.PAPER_MEDIUM
@@ -566,16 +566,16 @@ def test_serving_design_step_matches_oracle_chain(pkg, oracle):
 
 
 def test_serving_mixed_falls_back_to_fp64_and_certifies(pkg):
-    """High-contrast lineages run FP64 by policy; a mixed request that fails certification is
-    redone in FP64 from the mixed iterate, and the result is certified."""
+    """With an FP64 policy below Emin 1e-7, high-contrast lineages run FP64; a mixed request that
+    fails certification is redone in FP64 from the mixed iterate, and the result is certified."""
     sv = pkg.serve
     lin = sv.Lineage(n=24, seed=8, emin=1e-9, steps=2, tag="hi")
-    res = sv.Server(precision="mixed").run([sv.Arrival(0.0, lin)], realtime=False)
+    res = sv.Server(precision="mixed", fp64_below_emin=1e-7).run([sv.Arrival(0.0, lin)], realtime=False)
     assert [r.precision for r in res] == ["fp64", "fp64"] and all(r.status == 0 for r in res)
-    # forced onto the mixed path, this n=54, Emin=1e-9 design stalls near 2e-8 at the iteration cap
-    # (FP32 operator error amplified by the contrast); the FP64 redo certifies
+    # on the mixed path with alpha 0.5, this n=54, Emin=1e-9 design reaches the iteration cap near
+    # 2e-8; the FP64 redo certifies
     server = sv.Server(precision="mixed", fp64_below_emin=0.0)
-    lin = sv.Lineage(n=54, seed=1004, emin=1e-9, steps=1, tag="forced")
+    lin = sv.Lineage(n=54, seed=1004, emin=1e-9, steps=1, alpha=0.5, tag="forced")
     out = server.run([sv.Arrival(0.0, lin)], realtime=False)
     assert len(out) == 1 and server.fallbacks == 1
     assert out[0].precision == "fp64-fallback" and out[0].status == 0
@@ -599,3 +599,19 @@ def test_n96_mixed_and_fp64_certify_and_agree(pkg):
         assert st == 0 and all(i["relative_residual"] <= 1e-8 for i in infos), (prec, infos)
         out[prec] = op.effective_tensor(u).cpu().numpy()
     assert rel(out["mixed"], out["fp64"]) < 1e-7, rel(out["mixed"], out["fp64"])
+
+
+def test_serving_eta_alpha_runs_high_contrast_lineages_mixed(pkg):
+    """By default a mixed server runs every lineage mixed, with the eta-lookup alpha of its Emin
+    (13/16 at 1e-9), and its steps certify without an FP64 redo; the first step's C_H agrees with an
+    FP64 server's within the mixed tolerance."""
+    sv = pkg.serve
+    assert sv.eta_alpha(1e-9) == 13 / 16 and sv.eta_alpha(1e-4) == 9 / 16
+    lin = sv.Lineage(n=24, seed=8, emin=1e-9, steps=2, tag="hi")
+    server = sv.Server(precision="mixed")
+    res = server.run([sv.Arrival(0.0, lin)], realtime=False)
+    assert [r.precision for r in res] == ["mixed", "mixed"] and all(r.status == 0 for r in res)
+    assert server.fallbacks == 0
+    ref = sv.Server(precision="fp64").run([sv.Arrival(0.0, sv.Lineage(n=24, seed=8, emin=1e-9, steps=1, tag="f"))],
+                                         realtime=False)
+    assert rel(res[0].C, ref[0].C) < 1e-7

@@ -136,9 +136,12 @@ def test_design_updates_commit_only_after_certified_steps(pkg):
 
 def test_policy_and_oversized_requests(pkg):
     sv = pkg.serve
-    s = _fake_server(pkg, precision="mixed")
+    s = _fake_server(pkg, precision="mixed", fp64_below_emin=1e-7)
     out = s.run([sv.Arrival(0.0, sv.Lineage(n=16, seed=0, emin=1e-9, steps=1, tag="hi"))], realtime=False)
     assert out[0].precision == "fp64"  # Emin below the threshold runs in FP64
+    s = _fake_server(pkg, precision="mixed")
+    out = s.run([sv.Arrival(0.0, sv.Lineage(n=16, seed=0, emin=1e-9, steps=1, tag="hi"))], realtime=False)
+    assert out[0].precision == "mixed"  # by default every lineage runs mixed
     tiny = _fake_server(pkg, precision="mixed", hbm_budget=1024)
     with pytest.raises(RuntimeError, match="HBM budget"):
         tiny.run([sv.Arrival(0.0, sv.Homogenize(np.zeros((16, 16, 16)), 0.5, tag=0))], realtime=False)
