@@ -602,8 +602,12 @@ static int run_fz64(pgj_ctx* c, int loads, const GreenArgs& A, cudaStream_t s) {
   constexpr int WPB = fz64_warps<T>();
   const int warps = ((c->ns + 3) / 4) * c->n;  // per load
   const dim3 grid((warps + WPB - 1) / WPB, loads);
-  const char* e = std::getenv("PGJ_FZ64_MINB");  // default: three blocks per SM (register cap); 1: unbounded
-  if (e && e[0] == '1') k_fz64<T, WPB, 1><<<grid, WPB * 32, fz64_smem<T>(), s>>>(A);
+  // blocks per SM the register budget is sized for: default three; PGJ_FZ64_MINB = 1 (unbounded), 4, 6
+  const char* e = std::getenv("PGJ_FZ64_MINB");
+  const int minb = e ? std::atoi(e) : 3;
+  if (minb == 1) k_fz64<T, WPB, 1><<<grid, WPB * 32, fz64_smem<T>(), s>>>(A);
+  else if (minb == 4) k_fz64<T, WPB, 4><<<grid, WPB * 32, fz64_smem<T>(), s>>>(A);
+  else if (minb == 6) k_fz64<T, WPB, 6><<<grid, WPB * 32, fz64_smem<T>(), s>>>(A);
   else k_fz64<T, WPB, 3><<<grid, WPB * 32, fz64_smem<T>(), s>>>(A);
   return check_launch();
 }
@@ -618,6 +622,8 @@ static int set_smem_limits() {
   cudaFuncSetAttribute(k_ifx<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fz64<T, fz64_warps<T>(), 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fz64<T, fz64_warps<T>(), 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fz64<T, fz64_warps<T>(), 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fz64<T, fz64_warps<T>(), 6>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   return check_launch();
 }
 

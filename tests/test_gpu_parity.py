@@ -615,3 +615,25 @@ def test_serving_eta_alpha_runs_high_contrast_lineages_mixed(pkg):
     ref = sv.Server(precision="fp64").run([sv.Arrival(0.0, sv.Lineage(n=24, seed=8, emin=1e-9, steps=1, tag="f"))],
                                          realtime=False)
     assert rel(res[0].C, ref[0].C) < 1e-7
+
+
+@pytest.mark.parametrize("n,emin,alpha", [(16, 1e-6, 0.5), (32, 1e-9, 0.8125), (64, 1e-6, 0.5)])
+def test_mixed_flexible_beta_certifies_and_agrees(pkg, n, emin, alpha):
+    """The flexible (Polak-Ribiere) direction update of the FP32 recurrences certifies to 1e-8 and
+    gives C_H within the mixed tolerance of the FP64 solve; FP64 contexts refuse it."""
+    lam, mu = pkg.PAPER_MEDIUM
+    a = dev(pkg.baseline_design(n, 2, emin))
+    out = {}
+    for prec, flex in (("fp64", False), ("mixed", True)):
+        op = pkg.Operator(n, 6, lam, mu, precision=prec)
+        if flex:
+            op.set_flexible_beta(True)
+        op.set_material(a)
+        op.set_alpha(alpha)
+        u = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")
+        infos, st = op.solve(np.eye(6), 1e-8, u)
+        assert st == 0 and all(i["relative_residual"] <= 1e-8 for i in infos), (prec, infos)
+        out[prec] = op.effective_tensor(u).cpu().numpy()
+    assert rel(out["mixed"], out["fp64"]) < 1e-7
+    with pytest.raises(RuntimeError, match="unsupported"):
+        pkg.Operator(8, 6, lam, mu).set_flexible_beta(True)
