@@ -92,7 +92,9 @@ __device__ __forceinline__ void line64(cplx<T> (&v)[8], cplx<T>* L, int t, const
 // R64 (n = 64, 288 threads): x and y lines as register four-step transforms (line64); shared
 // memory holds 36 lines of 72 complex values (packed x lines, then per-warp transpose space) and
 // the n x nsp half-spectrum rows.
-template <typename T, typename U, int MODE, bool W4, bool R64>
+// FLEX: the flexible direction update (FP32 only) adds r_new . z_prev to the block sums; a separate
+// instantiation, so the plain forms keep their register budget (the runtime branch cost 3-6 us).
+template <typename T, typename U, int MODE, bool W4, bool R64, bool FLEX = false>
 __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -120,14 +122,14 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   const float* s32 = sizeof(T) == 4 ? A.scale32 + dsg * N3 + size_t(c) * nn * n + node0 : nullptr;  // coalesced
   T* packed = real_view<T>(b0);
   const int lpx = R64 ? kLine64 : n + 1;  // pitch of the packed x lines
-  double acc[3] = {0.0, 0.0, 0.0};
+  double acc[FLEX ? 3 : 2] = {};
   const double alpha = MODE == kSlabUpdate ? S.alpha : 0.0;
   const T a = T(alpha);
   // nodes whose loads are in flight together (the FP64 update keeps five doubles per node)
   constexpr int UNR = (MODE == kSlabUpdate && sizeof(T) == 8) ? 2 : 4;
   const T* pg = reinterpret_cast<const T*>(A.p) + off;
   const T* qg = reinterpret_cast<const T*>(A.q) + off;
-  const T* zg = A.flex ? reinterpret_cast<const T*>(A.zprev) + off : nullptr;
+  const T* zg = FLEX ? reinterpret_cast<const T*>(A.zprev) + off : nullptr;
   U* ug = reinterpret_cast<U*>(A.u) + off;
   const double* r64 = A.r64 + off64;
   for (int i0 = tid; i0 < nn; i0 += UNR * nthr) {
@@ -160,7 +162,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
           const double rd = double(rj);
           acc[0] += rd * rd;
           acc[1] += rd;
-          if (zg) acc[2] += rd * double(zg[k]);
+          if constexpr (FLEX) acc[FLEX ? 2 : 0] += rd * double(zg[k]);
         } else if (MODE == kSlabSync) {
           r[k] = rj;
         }
@@ -207,6 +209,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   C* sp = reinterpret_cast<C*>(A.spec) + ((size_t(load) * 3 + c) * n + z) * size_t(n) * nsp;
   if constexpr (R64) {
     // columns four per warp (nine warps), straight from the rows to the spectrum in global memory
+    // (staging the plane for one bulk store measured slower: 99 vs 93 us FP64, 51 vs 47 us FP32)
     const int col = 4 * warp + li;
     const bool valid = col < ns;
     C* L = b0 + (4 * warp + li) * kLine64;  // free once the split has read the packed lines
@@ -231,18 +234,19 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   const int nblk = 3 * n, blk = c + 3 * z;
   double* part = A.partials + size_t(load) * kPartialQ * kMaxPartials;
   if (MODE == kSlabUpdate) {
-    block_sum<3>(acc, red);
+    block_sum<FLEX ? 3 : 2>(acc, red);
     if (tid == 0) {
       part[blk] = acc[0];
       for (int cc = 0; cc < 3; ++cc) part[(1 + cc) * kMaxPartials + blk] = cc == c ? acc[1] : 0.0;
-      part[4 * kMaxPartials + blk] = acc[2];
+      if constexpr (FLEX) part[4 * kMaxPartials + blk] = acc[FLEX ? 2 : 0];
     }
     if (!last_block(&S.ticket[kTicketUpdate], nblk)) return;
     if (tid < 32) {
-      double v[5];
-      for (int k = 0; k < 5; ++k) v[k] = warp_sum_partials(part + k * kMaxPartials, nblk);
+      constexpr int NV = FLEX ? 5 : 4;
+      double v[5] = {};
+      for (int k = 0; k < NV; ++k) v[k] = warp_sum_partials(part + k * kMaxPartials, nblk);
       if (tid == 0) {
-        S.rz_cross = v[4];
+        if constexpr (FLEX) S.rz_cross = v[4];
         // same bookkeeping as the unfused update (k_update_ur)
         const double res2 = v[0];
         const bool finite = isfinite(res2);
@@ -274,7 +278,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
 }
 
 // ----------------------------------------------------------------------------------------- ifxy
-template <typename T, bool W4, bool R64>
+template <typename T, bool W4, bool R64, bool FLEX = false>
 __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -301,15 +305,37 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
   C* res;
   C* oth;
   if constexpr (R64) {
-    // inverse y of four columns per warp straight from global memory into the rows (b1)
+    // inverse y of four columns per warp into the rows (b1). FP64: the slab's half spectrum (n rows
+    // of nsp, contiguous in global memory) first arrives in b1 as one bulk copy (56 vs 58 us); FP32
+    // reads the columns straight from global memory (31 vs 33 us)
+    constexpr bool kBulk = sizeof(T) == 8;
+    __shared__ alignas(8) uint64_t sbar;
+    if (kBulk) {
+      if (tid == 0) {
+        mbar_init(&sbar, 1);
+        fence_mbar_init();
+      }
+      __syncthreads();
+      if (tid == 0) {
+        const unsigned pbytes = unsigned(size_t(n) * nsp * sizeof(C));
+        mbar_expect_tx(&sbar, pbytes);
+        tma_row(b1, sp, pbytes, &sbar);
+      }
+      const bool arrived = mbar_wait(&sbar, 0);  // bounded; every thread observes the arrival
+      if (__syncthreads_or(!arrived)) {
+        if (tid == 0) atomicExch(&A.counters[2], 1);  // reported as PGJ_ERR_TIMEOUT
+        return;
+      }
+    }
+    const C* src = kBulk ? b1 : sp;
     const int col = 4 * warp + li;
     const bool valid = col < ns;
     C* L = b0 + (4 * warp + li) * kLine64;
     C v[8];
     const C zero = cmk<C>(0.0, 0.0);
 #pragma unroll
-    for (int k1 = 0; k1 < 8; ++k1) v[k1] = valid ? sp[size_t(t8 + 8 * k1) * nsp + col] : zero;
-    line64<T>(v, L, t8, tw, true);
+    for (int k1 = 0; k1 < 8; ++k1) v[k1] = valid ? src[(t8 + 8 * k1) * nsp + col] : zero;
+    line64<T>(v, L, t8, tw, true);  // its warp barriers order the column reads before the writes
     if (valid) {
 #pragma unroll
       for (int b = 0; b < 8; ++b) b1[(t8 + 8 * b) * nsp + col] = v[b];
@@ -400,7 +426,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
         const T w = wv[2 * ((y >> 1) * lpx + x) + (y & 1)];
         const T zv = T(sv[j]) * w - m;
         p[size_t(KS) * i] = A.init ? zv : zv + beta * pv[j];
-        if (A.flex) reinterpret_cast<T*>(A.zprev)[off + size_t(KS) * i] = zv;
+        if constexpr (FLEX) reinterpret_cast<T*>(A.zprev)[off + size_t(KS) * i] = zv;
       }
     }
   }
@@ -428,12 +454,12 @@ bool slab_fits(const pgj_ctx* c) {
   return slab_smem(c->n, nsp, tsz) <= 110 * 1024;  // two blocks per SM
 }
 
-template <typename T, typename U, bool W4, bool R64>
+template <typename T, typename U, bool W4, bool R64, bool FLEX = false>
 static void set_fxy_smem(int lim) {
-  cudaFuncSetAttribute(k_fxy<T, U, kSlabUpdate, W4, R64>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<T, U, kSlabInit, W4, R64>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_fxy<T, U, kSlabSync, W4, R64>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  cudaFuncSetAttribute(k_ifxy<T, W4, R64>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<T, U, kSlabUpdate, W4, R64, FLEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<T, U, kSlabInit, W4, R64, FLEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_fxy<T, U, kSlabSync, W4, R64, FLEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  cudaFuncSetAttribute(k_ifxy<T, W4, R64, FLEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
 }
 
 int prepare_slab_kernels() {
@@ -443,6 +469,9 @@ int prepare_slab_kernels() {
   set_fxy_smem<float, float, false, false>(lim);
   set_fxy_smem<float, float, true, false>(lim);
   set_fxy_smem<float, float, true, true>(lim);
+  set_fxy_smem<float, float, false, false, true>(lim);
+  set_fxy_smem<float, float, true, false, true>(lim);
+  set_fxy_smem<float, float, true, true, true>(lim);
   return check_launch();
 }
 
@@ -479,12 +508,12 @@ static SlabArgs slab_args(pgj_ctx* c, int loads, int prec) {
 }
 
 // mode: kSlabUpdate (u in `u`: FP64 x, or the FP32 correction d), kSlabInit, kSlabSync
-template <typename T, typename U, bool W4, bool R64>
+template <typename T, typename U, bool W4, bool R64, bool FLEX = false>
 static void fxy_kernel(int mode, dim3 grid, int thr, size_t smem, cudaStream_t s, const SlabArgs& A) {
   switch (mode) {
-    case kSlabUpdate: k_fxy<T, U, kSlabUpdate, W4, R64><<<grid, thr, smem, s>>>(A); break;
-    case kSlabInit: k_fxy<T, U, kSlabInit, W4, R64><<<grid, thr, smem, s>>>(A); break;
-    default: k_fxy<T, U, kSlabSync, W4, R64><<<grid, thr, smem, s>>>(A); break;
+    case kSlabUpdate: k_fxy<T, U, kSlabUpdate, W4, R64, FLEX><<<grid, thr, smem, s>>>(A); break;
+    case kSlabInit: k_fxy<T, U, kSlabInit, W4, R64, FLEX><<<grid, thr, smem, s>>>(A); break;
+    default: k_fxy<T, U, kSlabSync, W4, R64, FLEX><<<grid, thr, smem, s>>>(A); break;
   }
 }
 
@@ -496,7 +525,11 @@ int launch_fxy(pgj_ctx* c, int loads, int prec, int mode, void* u, cudaStream_t 
   const int thr = slab_threads(c);
   const bool r64 = slab_r64(c, prec, thr);
   const size_t smem = r64 ? slab_smem64(A.nsp, tsz) : slab_smem(A.n, A.nsp, tsz);
-  if (prec == PGJ_FP32) {
+  if (prec == PGJ_FP32 && A.flex) {
+    if (r64) fxy_kernel<float, float, true, true, true>(mode, grid, thr, smem, s, A);
+    else if (slab_w4(prec, thr)) fxy_kernel<float, float, true, false, true>(mode, grid, thr, smem, s, A);
+    else fxy_kernel<float, float, false, false, true>(mode, grid, thr, smem, s, A);
+  } else if (prec == PGJ_FP32) {
     if (r64) fxy_kernel<float, float, true, true>(mode, grid, thr, smem, s, A);
     else if (slab_w4(prec, thr)) fxy_kernel<float, float, true, false>(mode, grid, thr, smem, s, A);
     else fxy_kernel<float, float, false, false>(mode, grid, thr, smem, s, A);
@@ -518,7 +551,11 @@ int launch_ifxy(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, cuda
   const int thr = slab_threads(c);
   const bool r64 = slab_r64(c, prec, thr);
   const size_t smem = r64 ? slab_smem64(A.nsp, tsz) : slab_smem(A.n, A.nsp, tsz);
-  if (prec == PGJ_FP32) {
+  if (prec == PGJ_FP32 && A.flex) {
+    if (r64) k_ifxy<float, true, true, true><<<grid, thr, smem, s>>>(A);
+    else if (slab_w4(prec, thr)) k_ifxy<float, true, false, true><<<grid, thr, smem, s>>>(A);
+    else k_ifxy<float, false, false, true><<<grid, thr, smem, s>>>(A);
+  } else if (prec == PGJ_FP32) {
     if (r64) k_ifxy<float, true, true><<<grid, thr, smem, s>>>(A);
     else if (slab_w4(prec, thr)) k_ifxy<float, true, false><<<grid, thr, smem, s>>>(A);
     else k_ifxy<float, false, false><<<grid, thr, smem, s>>>(A);

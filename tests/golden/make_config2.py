@@ -14,7 +14,10 @@ tests' count tolerances are stated against it.
 
 Grids: n = 32, alpha in {0, 0.5, 1} x Emin/E0 in {1e-4, 1e-6, 1e-9} x seeds 0..4 (45 cases),
 n = 64, alpha = 0.5 x Emin/E0 in {1e-4, 1e-6, 1e-9}, seed 0 (3 cases), and one high-contrast case
-that reaches the iteration cap, n = 54, alpha 0.5, Emin/E0 1e-9, seed 0. The n = 64 cases take
+that reaches the iteration cap, n = 54, alpha 0.5, Emin/E0 1e-9, seed 0 (``--set all``, written to
+config2.json). ``--set config3 --orders a --out tests/golden/config3.json`` writes the mixed-precision
+grids' FP64 references: n = 96 at Emin/E0 1e-6 and 1e-9 and n = 128 at 1e-6, alpha 0.5, seed 0
+(hours of host time each). The n = 64 cases take
 about an hour of single-core time each, so the script runs a spawn-started process pool and
 checkpoints finished runs to ``--checkpoint`` so that an interrupted run resumes.
 Nothing here runs on the GPU or reads the reference tree.
@@ -44,6 +47,9 @@ def cases(which: str):
         # high contrast at alpha 0.5: the device FP64 recurrence reaches the 4000-iteration cap here;
         # the oracle decides whether the reference would too
         out.append((54, 0.5, 1e-9, 0))
+    if which == "config3":
+        # the mixed-precision grids: the FP64 oracle's C_H is what the mixed results are held to
+        out += [(96, 0.5, 1e-6, 0), (96, 0.5, 1e-9, 0), (128, 0.5, 1e-6, 0)]
     if which in ("all", "n32"):
         for alpha in ALPHAS:
             for emin in EMINS:
@@ -102,7 +108,7 @@ def merge(records: list[dict]) -> dict:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workers", type=int, default=max(1, (os.cpu_count() or 2) - 1))
-    ap.add_argument("--set", default="all", choices=("all", "n32", "n64", "cap"))
+    ap.add_argument("--set", default="all", choices=("all", "n32", "n64", "cap", "config3"))
     ap.add_argument("--checkpoint", default="/tmp/pgj_config2_checkpoint.jsonl")
     ap.add_argument("--out", default=str(HERE / "config2.json"))
     ap.add_argument("--merge-only", action="store_true", help="write the fixture from the checkpoint, run nothing")
@@ -131,7 +137,7 @@ def main():
 
     merged = merge(done)
     Path(args.out).write_text(json.dumps(dict(
-        source="tests/golden/make_config2.py (CPU oracle, orders a and b)",
+        source=f"tests/golden/make_config2.py --set {args.set} (CPU oracle, orders {args.orders})",
         physics=dict(E0=1.0, nu=0.3, p=3, vf=0.35, sigma="n/16", width=0.1, rtol=1e-8),
         cases=merged), indent=1) + "\n")
     print(f"wrote {len(merged)} cases to {args.out}")
