@@ -160,11 +160,12 @@ int pgj_set_mixed_mode(pgj_ctx* ctx, int mode, double delta);
  * contrast, and a larger cap lets it certify where the FP64 recurrence needs most of the 4000. */
 int pgj_set_iteration_cap(pgj_ctx* ctx, int cap);
 int pgj_iteration_cap(pgj_ctx* ctx);
-/* Direction update of the FP32 recurrences of a slab-fused PGJ_FP32 context (no reference
- * counterpart; FP64 contexts keep the reference's beta = r.z / r_prev.z_prev): 1 selects the flexible
- * (Polak-Ribiere) form beta = r.(z - z_prev) / r_prev.z_prev, which keeps the new direction locally
- * orthogonal when the FP32 preconditioner apply is inexact; it stores z for the next iteration.
- * PGJ_ERR_UNSUPPORTED for other contexts. Default 0. */
+/* Direction update of the FP32 recurrences of a PGJ_FP32 context (no reference counterpart; FP64
+ * contexts keep the reference's beta = r.z / r_prev.z_prev): 1 selects the flexible (Polak-Ribiere)
+ * form beta = r.(z - z_prev) / r_prev.z_prev, which keeps the new direction locally orthogonal when
+ * the FP32 preconditioner apply is inexact (the slab-fused iteration stores z for the next
+ * iteration; the step-by-step one reads it back from the last Green output). PGJ_ERR_UNSUPPORTED for
+ * PGJ_FP64 contexts. Default 0. */
 int pgj_set_flexible_beta(pgj_ctx* ctx, int on);
 /* Arithmetic of the recurrence operator of a PGJ_FP32 context (no reference counterpart): 0 (default)
  * FP32; 1 FP64 element actions and node sums on the FP32 vectors, for high-contrast designs (weak
@@ -180,7 +181,8 @@ long long pgj_last_launches(pgj_ctx* ctx);
 /* Measurement hook (no reference counterpart; the reference times stages with CUDA events,
  * exp/asg_gpu_resident_20261103/run.py:29-53): starts a zero-start solve of `loads` macros and
  * times each kernel of the PCG iteration separately with CUDA events on `stream`, over `reps`
- * iterations. Writes PGJ_PROFILE_KERNELS mean durations (ms) and algorithmic bytes per launch
+ * back-to-back launches of that kernel (after two warm launches; the values drift, the work does
+ * not). Writes PGJ_PROFILE_KERNELS mean durations (ms) and algorithmic bytes per launch
  * (HOST arrays) in the order: operator, update_ur, fft_x, fft_y, fft_z+symbol, ifft_y, ifft_x,
  * update_p. Leaves the context's iterate undefined (the next pgj_solve starts from its u). */
 #define PGJ_PROFILE_KERNELS 8

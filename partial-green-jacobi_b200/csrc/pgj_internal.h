@@ -140,7 +140,8 @@ struct pgj_ctx {
 
 namespace pgj {
 // operator (pgj_operator.cu)
-// planar_plain: plain mode on the component-planar FP32 layout of a slab-fused context (the tuner)
+// planar_plain: plain mode writing q component-planar, as the recurrence operator of a slab-fused FP32
+// context does (the tuner)
 int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, void* out, const double* f,
                    const int32_t* active_ext, cudaStream_t s, const LoadScalars* rel_flags = nullptr,
                    bool planar_plain = false);

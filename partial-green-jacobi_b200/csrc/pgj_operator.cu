@@ -35,58 +35,36 @@ __device__ __forceinline__ void cp_wait_all() { asm volatile("cp.async.wait_grou
 __device__ __forceinline__ void cp_wait_one() { asm volatile("cp.async.wait_group 1;\n" ::); }
 
 // The rows of one plane issued by the lanes of one warp in parallel (lane r: rows r, r+32, ...):
-// lane 0 arms the mbarrier for all rows first. Called by all 32 lanes of the warp. Interleaved
-// vectors (cstride 0): one copy per node row of 3n values, landing as [row][x][component].
-// Component-planar vectors (components cstride apart in global memory): the plane's rows of one
-// component are consecutive in global memory, so each component is one copy of `rows` rows (two
-// where the tile wraps around the periodic y edge), landing as [component][row][x].
-template <typename T>
-__device__ __forceinline__ void plane_copy(T* buf, const T* in, int pz, int y0, int rows, int n, uint64_t* bar,
-                                           size_t cstride, int k) {
-  if (cstride == 0) {
-    int y = (y0 - 1 + k) % n;
-    if (y < 0) y += n;
-    tma_row(buf + k * 3 * n, in + (size_t(pz) * n + y) * size_t(3 * n), unsigned(3 * n * sizeof(T)), bar);
-    return;
-  }
-  // planar: k = 3 c + part. Rows r = 0..rows-1 are y = (y0 - 1 + r) mod n; they break into at most
-  // three contiguous runs (rows <= n + 2), and `part` is the run this call copies.
-  const int c = k / 3, part = k - 3 * c;
-  int r = 0;
-  for (int p = 0; r < rows; ++p) {
-    int y = (y0 - 1 + r) % n;
-    if (y < 0) y += n;
-    const int len = min(rows - r, n - y);
-    if (p == part) {
-      tma_row(buf + (size_t(c) * rows + r) * n, in + c * cstride + (size_t(pz) * n + y) * size_t(n),
-              unsigned(len * n * sizeof(T)), bar);
-      return;
-    }
-    r += len;
-  }
-}
-
+// lane 0 arms the mbarrier for all rows first. Called by all 32 lanes of the warp. One copy per node
+// row of 3n interleaved values, landing as [row][x][component]. (The component-planar FP32 vectors
+// of slab-fused contexts are the recurrence's r, d and q; the operator's input p stays interleaved:
+// staging a planar p as three component copies per plane measured 59.5 against 46.0 us.)
 template <typename T>
 __device__ __forceinline__ void tma_plane_warp(T* buf, const T* in, int pz, int y0, int rows, int n, uint64_t* bar,
-                                               int lane, size_t cstride) {
+                                               int lane) {
   const unsigned rowbytes = unsigned(3 * n * sizeof(T));
   if (lane == 0) {
     fence_proxy_async();
     mbar_expect_tx(bar, rowbytes * rows);
   }
   __syncwarp();
-  const int copies = cstride == 0 ? rows : 9;
-  for (int k = lane; k < copies; k += 32) plane_copy(buf, in, pz, y0, rows, n, bar, cstride, k);
+  for (int r = lane; r < rows; r += 32) {
+    int y = (y0 - 1 + r) % n;
+    if (y < 0) y += n;
+    tma_row(buf + r * 3 * n, in + (size_t(pz) * n + y) * size_t(3 * n), rowbytes, bar);
+  }
 }
 
 template <typename T>
-__device__ __forceinline__ void tma_plane(T* buf, const T* in, int pz, int y0, int rows, int n, uint64_t* bar,
-                                          size_t cstride) {
+__device__ __forceinline__ void tma_plane(T* buf, const T* in, int pz, int y0, int rows, int n, uint64_t* bar) {
   const unsigned rowbytes = unsigned(3 * n * sizeof(T));
   fence_proxy_async();
   mbar_expect_tx(bar, rowbytes * rows);
-  const int copies = cstride == 0 ? rows : 9;
-  for (int k = 0; k < copies; ++k) plane_copy(buf, in, pz, y0, rows, n, bar, cstride, k);
+  for (int r = 0; r < rows; ++r) {
+    int y = (y0 - 1 + r) % n;
+    if (y < 0) y += n;
+    tma_row(buf + r * 3 * n, in + (size_t(pz) * n + y) * size_t(3 * n), rowbytes, bar);
+  }
 }
 
 StencilGeom stencil_geom_shape(int n, int ty, int zc, int stages, int occ) {
@@ -138,8 +116,7 @@ StencilGeom stencil_geom(int n, int loads) {
 }
 
 template <typename T>
-__device__ __forceinline__ void stage_plane(T* buf, const T* in, int pz, int y0, int rows, int n, int tid, int nthr,
-                                            size_t cstride) {
+__device__ __forceinline__ void stage_plane(T* buf, const T* in, int pz, int y0, int rows, int n, int tid, int nthr) {
   const int rowlen = 3 * n;
   const int total = rows * rowlen;
   for (int i = tid; i < total; i += nthr) {
@@ -147,12 +124,7 @@ __device__ __forceinline__ void stage_plane(T* buf, const T* in, int pz, int y0,
     const int rem = i - row * rowlen;
     int y = (y0 - 1 + row) % n;
     if (y < 0) y += n;
-    if (cstride == 0) {
-      cp_async(buf + i, in + (size_t(pz) * n + y) * size_t(rowlen) + rem);
-    } else {  // component-planar: the buffer is [component][row][x]
-      const int c = rem / n, x = rem - c * n;
-      cp_async(buf + (size_t(c) * rows + row) * n + x, in + c * cstride + (size_t(pz) * n + y) * size_t(n) + x);
-    }
+    cp_async(buf + i, in + (size_t(pz) * n + y) * size_t(rowlen) + rem);
   }
   cp_commit();
 }
@@ -185,24 +157,16 @@ struct Tri<float> {
   }
 };
 
-// Read the 4 nodes of the face (x..x+1, row..row+1) from a staged plane and form the face modes
-// F[f], f = mx + 2 my: F[0] = sum, F[1] = x-difference, F[2] = y-difference, F[3] = both.
-// PL: the staged plane is component-planar ([component][row][x], components cs = rows * n apart)
-// instead of interleaved ([row][x][component]).
-template <bool PL, typename T>
-__device__ __forceinline__ Tri<T> node_at(const T* row, int x, int cs) {
-  if constexpr (PL) return Tri<T>::make(row[x], row[cs + x], row[2 * cs + x]);
-  else return Tri<T>::load(row + 3 * x);
-}
-
-template <bool PL, typename T>
-__device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, int rows, Tri<T> (&F)[4], Tri<T>& own) {
+// Read the 4 nodes of the face (x..x+1, row..row+1) from a staged plane ([row][x][component]) and
+// form the face modes F[f], f = mx + 2 my: F[0] = sum, F[1] = x-difference, F[2] = y-difference,
+// F[3] = both.
+template <typename T>
+__device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, Tri<T> (&F)[4], Tri<T>& own) {
   const int xp = (x + 1 == n) ? 0 : x + 1;
-  const int rs = PL ? n : 3 * n, cs = rows * n;  // row stride; component stride (planar)
-  const T* r0 = buf + row * rs;
-  const T* r1 = r0 + rs;
-  const Tri<T> u00 = node_at<PL>(r0, x, cs), u10 = node_at<PL>(r0, xp, cs);
-  const Tri<T> u01 = node_at<PL>(r1, x, cs), u11 = node_at<PL>(r1, xp, cs);
+  const T* r0 = buf + row * 3 * n;
+  const T* r1 = r0 + 3 * n;
+  const Tri<T> u00 = Tri<T>::load(r0 + 3 * x), u10 = Tri<T>::load(r0 + 3 * xp);
+  const Tri<T> u01 = Tri<T>::load(r1 + 3 * x), u11 = Tri<T>::load(r1 + 3 * xp);
   own = u00;
   const Tri<T> sx0 = u10 + u00, dx0 = u10 - u00, sx1 = u11 + u01, dx1 = u11 - u01;
   F[0] = sx1 + sx0;
@@ -213,17 +177,14 @@ __device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, 
 
 // The same face modes one component at a time (the FP64 loop), in the compute type R (the staged
 // values are of the storage type T: FP64, or FP32 for the FP64-arithmetic form of the FP32 operator).
-template <bool PL, typename T, typename R>
-__device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, int rows, R (&F)[4][3], R (&own)[3]) {
+template <typename T, typename R>
+__device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, R (&F)[4][3], R (&own)[3]) {
   const int xp = (x + 1 == n) ? 0 : x + 1;
-  const int rs = PL ? n : 3 * n;               // row stride
-  const T* r0 = buf + row * rs;
-  const T* r1 = r0 + rs;
-  const int xs = PL ? 1 : 3, cs = PL ? rows * n : 1;  // element strides of x and of the component
+  const T* r0 = buf + row * 3 * n;
+  const T* r1 = r0 + 3 * n;
 #pragma unroll
   for (int c = 0; c < 3; ++c) {
-    const R u00 = R(r0[xs * x + cs * c]), u10 = R(r0[xs * xp + cs * c]), u01 = R(r1[xs * x + cs * c]),
-            u11 = R(r1[xs * xp + cs * c]);
+    const R u00 = R(r0[3 * x + c]), u10 = R(r0[3 * xp + c]), u01 = R(r1[3 * x + c]), u11 = R(r1[3 * xp + c]);
     own[c] = u00;
     const R sx0 = u10 + u00, dx0 = u10 - u00, sx1 = u11 + u01, dx1 = u11 - u01;
     F[0][c] = sx1 + sx0;
@@ -238,8 +199,9 @@ __device__ __forceinline__ void face_modes(const T* buf, int row, int x, int n, 
 // arithmetic type (R = double with T = float: FP32 vectors, FP64 element actions and node sums, for
 // high-contrast designs whose FP32 node sums cancel).
 //
-// PL: p and q of this launch are component-planar, (3, N) per load (the FP32 recurrence vectors of a
-// slab-fused mixed context); otherwise node-major with the components interleaved.
+// PL: q of this launch is written component-planar, (3, N) per load (the FP32 recurrence vector of a
+// slab-fused mixed context, read per component by the slab kernels); otherwise node-major with the
+// components interleaved. p is read interleaved either way.
 template <typename T, int MODE, int OCC, typename R = T, bool PL = false>
 __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const StencilArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -249,7 +211,6 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   const int load = blockIdx.z;
   const int nblk = gridDim.x * gridDim.y, blk = blockIdx.x + gridDim.x * blockIdx.y;
   const size_t N = size_t(n) * n * n;
-  const size_t cs = PL ? N : 0;  // global distance between the components of a node (0: interleaved)
   const int y0 = blockIdx.x * TY, z0 = blockIdx.y * A.zc;
   const int zc = min(A.zc, n - z0);
   const int ey = y0 - 1 + ty;
@@ -281,13 +242,11 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   const int planevals = (TY + 2) * 3 * n;
   const int nt = n * (TY + 1);
   T* bufs = reinterpret_cast<T*>(smem_raw);
-  // corner exchange in the arithmetic type: [slot][corner 10 / 01 / 11][thread][3], four slots by
-  // step mod 4 for the FP32 loop (one barrier per two steps), two by step parity for the FP64 loop
-  // (n is even, so the plane buffers end 8-byte aligned)
+  // corner exchange in the arithmetic type, double-buffered by step parity:
+  // [parity][corner 10 / 01 / 11][thread][3] (n is even, so the plane buffers end 8-byte aligned)
   R* xch = reinterpret_cast<R*>(bufs + NS * planevals);
   const int xsz = 3 * nt * 3;
-  constexpr int XSLOTS = sizeof(R) == 4 ? 4 : 2;
-  double* red = reinterpret_cast<double*>(xch + XSLOTS * xsz + 2);  // 32 * 4, 16-byte padded
+  double* red = reinterpret_cast<double*>(xch + 2 * xsz + 2);  // 32 * 4, 16-byte padded
   red = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(red) + 15) & ~uintptr_t(15));
   uint64_t* bars = reinterpret_cast<uint64_t*>(red + 32 * 4);  // NS mbarriers (TMA staging)
   const bool tma = A.tma != 0;
@@ -303,11 +262,11 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
     __syncthreads();
     if (tid == 0)
       for (int j = 0; j < NS && j < nplanes; ++j)
-        tma_plane(bufs + j * planevals, in, (z0 - 1 + j + n) % n, y0, TY + 2, n, &bars[j], cs);
+        tma_plane(bufs + j * planevals, in, (z0 - 1 + j + n) % n, y0, TY + 2, n, &bars[j]);
     bad = !mbar_wait(&bars[0], 0);  // every thread observes the arrival (acquire)
   } else {
-    stage_plane(bufs, in, (z0 - 1 + n) % n, y0, TY + 2, n, tid, nthr, cs);
-    stage_plane(bufs + planevals, in, z0 % n, y0, TY + 2, n, tid, nthr, cs);
+    stage_plane(bufs, in, (z0 - 1 + n) % n, y0, TY + 2, n, tid, nthr);
+    stage_plane(bufs + planevals, in, z0 % n, y0, TY + 2, n, tid, nthr);
     cp_wait_one();
     __syncthreads();
   }
@@ -315,18 +274,20 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   if constexpr (sizeof(R) == 4) {
     // FP32: packed-pair arithmetic (Tri) and two z-steps per loop trip, which removes the copies of
     // the carried face modes; 47 vs 51 us at n = 64, 6 loads. FP64 keeps the one-step form below:
-    // the same restructuring made it slower (64 vs 61 us).
+    // the same restructuring made it slower (64 vs 61 us). One block barrier per step: sharing one
+    // barrier between the two steps of a trip (four exchange slots) halved the barrier stalls but
+    // measured 2 us slower (46.1 vs 43.7 us), with the own node values of two planes live.
     // lower-face modes, upper-plane carry and own node value of the plane below, in two sets that
     // swap roles every z-step (no copies at the loop edge)
     Tri<T> FA[4], UA[4], ownA, FB[4], UB[4], ownB;
-    face_modes<PL>(bufs, ty, tx, n, TY + 2, FA, ownB);
+    face_modes(bufs, ty, tx, n, FA, ownB);
     if (tma) {
       // buffer 0 is free once every thread has read plane 0
       if (__syncthreads_or(bad)) {
         if (tid == 0 && A.err) atomicExch(A.err, 1);
         return;
       }
-      if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0], cs);
+      if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0]);
     }
 #pragma unroll
     for (int f = 0; f < 4; ++f) UA[f] = Tri<T>::make(T(0), T(0), T(0));
@@ -352,29 +313,25 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
 
     // One element plane s: F0 / Up / own0 hold the lower face modes, the carry from the element
     // below and the own node value of node plane ez; F1 / U / own1 receive those of the next plane.
-    // The lower face of the element (node plane ez) goes out as its four corner nodes: the thread
-    // keeps the (x, y) corner in c00 and hands (x+1, y), (x, y+1), (x+1, y+1) to their owners through
-    // the exchange buffer of the step. The plane buffer is not released here: two steps share one
-    // block barrier (publish).
-    auto compute = [&](int s, const Tri<T> (&F0)[4], const Tri<T> (&Up)[4], Tri<T> (&F1)[4], Tri<T> (&U)[4],
-                       Tri<T>& own1, Tri<T>& c00, int pb, unsigned ppar) {
+    // Returns false when a bounded wait gave up (the block then leaves).
+    auto step = [&](int s, const Tri<T> (&F0)[4], const Tri<T> (&Up)[4], const Tri<T>& own0, Tri<T> (&F1)[4],
+                    Tri<T> (&U)[4], Tri<T>& own1) -> bool {
+      const int ez = z0 - 1 + s;           // element plane
       const T ae = T(a_next);
       if (s < zc) {
         za = za + 1 == n ? 0 : za + 1;
         a_next = __ldg(arow + size_t(za) * aplane);
       }
-      T* cur = bufs + pb * planevals;
+      T* cur = bufs + jb * planevals;
       if (tma) {
-        bad = bad || !mbar_wait(&bars[pb], ppar);
+        bad = bad || !mbar_wait(&bars[jb], jpar);
       } else {
-        // cp.async staging (rows not 16-byte multiples): two buffers, plane s + 1 is complete after
-        // the wait, and the barrier tells that every thread has read plane s before plane s + 2
-        // overwrites its buffer
         cp_wait_all();
         __syncthreads();
-        if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr, cs);
+        if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
       }
-      face_modes<PL>(cur, ty, tx, n, TY + 2, F1, own1);
+
+      face_modes(cur, ty, tx, n, F1, own1);
       // element modes: z level
       T Q[8][3];
 #pragma unroll
@@ -394,8 +351,11 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
         U[f] = lo + hi;
         G[f] = (lo - hi) + Up[f];
       }
+      // lower face of the element (node plane ez) as its four corner nodes: this thread keeps the
+      // (x, y) corner and hands (x+1, y), (x, y+1), (x+1, y+1) to their owners through shared memory
+      Tri<T> c00;
+      T* xb = xch + (s & 1) * xsz;
       if (s >= 1) {
-        T* xb = xch + (s & 3) * xsz;
         const Tri<T> ly0 = G[0] - G[2], ly1 = G[1] - G[3];
         const Tri<T> uy0 = G[0] + G[2], uy1 = G[1] + G[3];
         c00 = ly0 - ly1;
@@ -403,94 +363,68 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
         (uy0 - uy1).store(xb + (1 * nt + tme) * 3);
         (uy0 + uy1).store(xb + (2 * nt + tme) * 3);
       }
-    };
-    // The node row of plane ez = z0 - 1 + s (s >= 1) after the barrier that published step s.
-    auto output = [&](int s, const Tri<T>& c00, const Tri<T>& own0) {
-      const T* xb = xch + (s & 3) * xsz;
-      const int ez = z0 - 1 + s;
-      const Tri<T> qx = ((c00 + Tri<T>::load(xb + (0 * nt + tl) * 3)) + Tri<T>::load(xb + (1 * nt + tb) * 3)) +
-                        Tri<T>::load(xb + (2 * nt + tbl) * 3);
-      const size_t node = (size_t(ez) * n + ey) * n + tx;
-      T* o = out + (PL ? node : 3 * node);
-      // FP32 never runs the residual mode (the host rejects it); the branch is kept because the
-      // build without it allocates registers differently and measured 0.6 us slower
-      if (MODE == kResidual) {
-        const double* fl = A.f + size_t(load) * 3 * N + 3 * node;
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-          const double rv = fl[c] - double(qx.get(c));
-          o[c] = T(rv);
-          acc[0] += rv * rv;
-          acc[1 + c] += rv;
-        }
-      } else {
-        if constexpr (PL) {
-          o[0] = qx.get(0); o[N] = qx.get(1); o[2 * N] = qx.get(2);
-        } else {
-          qx.store(o);
-        }
-        if (MODE == kPCG) {
-#pragma unroll
-          for (int c = 0; c < 3; ++c) acc[0] += double(own0.get(c)) * double(qx.get(c));
-        }
+      // one barrier per step: corners published, plane jb fully read, timeouts agreed on
+      if (__syncthreads_or(bad)) {
+        if (tid == 0 && A.err) atomicExch(A.err, 1);
+        return false;
       }
-    };
-    // refill: the buffer of the plane read at step s takes plane s + 1 + NS (node plane zr)
-    auto refill = [&](int s, int pb) {
       if (tma && s + 1 + NS < nplanes) {
         // warp 0 refills (its lanes issue the rows in parallel); a block of fewer than 32 threads
         // has no full warp, and thread 0 issues the rows alone
         if (full_warp0) {
-          if (tid < 32) tma_plane_warp(bufs + pb * planevals, in, zr, y0, TY + 2, n, &bars[pb], tid, cs);
+          if (tid < 32) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid);
         } else if (tid == 0) {
-          tma_plane(bufs + pb * planevals, in, zr, y0, TY + 2, n, &bars[pb], cs);
+          tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb]);
         }
       }
-      zr = zr + 1 == n ? 0 : zr + 1;
-    };
-    // Two z-steps per loop trip with the register sets swapped (the carries stay where they were
-    // written) and ONE block barrier per trip: the exchange buffers rotate over four slots (s mod 4),
-    // so a trip writes two slots while the slots read in the trip before are no longer in use, and
-    // the two plane buffers read in the trip are released together after the barrier.
-    // Node values: own of plane s (the lower face of step s) is in ownA at even steps; step s writes
-    // the upper face's (plane s + 1) into ownB, step s + 1 plane s + 2's into ownA.
-    Tri<T> cA = Tri<T>::make(T(0), T(0), T(0)), cB = cA;
-    for (int s = 0; s <= zc; s += 2) {
-      const bool two = s + 1 <= zc;
-      const int pb0 = jb;
-      const unsigned pp0 = jpar;
       if (++jb == NS) { jb = 0; jpar ^= 1u; }
-      compute(s, FA, UA, FB, UB, ownB, cA, pb0, pp0);
-      const Tri<T> own_s = ownA;  // plane s, for step s's output after compute(s + 1) rewrote ownA
-      int pb1 = 0;
-      if (two) {
-        pb1 = jb;
-        const unsigned pp1 = jpar;
-        if (++jb == NS) { jb = 0; jpar ^= 1u; }
-        compute(s + 1, FB, UB, FA, UA, ownA, cB, pb1, pp1);
+      zr = zr + 1 == n ? 0 : zr + 1;
+      if (s >= 1 && out_row) {
+        const Tri<T> qx = ((c00 + Tri<T>::load(xb + (0 * nt + tl) * 3)) + Tri<T>::load(xb + (1 * nt + tb) * 3)) +
+                          Tri<T>::load(xb + (2 * nt + tbl) * 3);
+        const size_t node = (size_t(ez) * n + ey) * n + tx;
+        T* o = out + (PL ? node : 3 * node);
+        // FP32 never runs the residual mode (the host rejects it); the branch is kept because the
+        // build without it allocates registers differently and measured 0.6 us slower
+        if (MODE == kResidual) {
+          const double* fl = A.f + size_t(load) * 3 * N + 3 * node;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            const double rv = fl[c] - double(qx.get(c));
+            o[c] = T(rv);
+            acc[0] += rv * rv;
+            acc[1 + c] += rv;
+          }
+        } else {
+          if constexpr (PL) {
+            o[0] = qx.get(0); o[N] = qx.get(1); o[2 * N] = qx.get(2);
+          } else {
+            qx.store(o);
+          }
+          if (MODE == kPCG) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) acc[0] += double(own0.get(c)) * double(qx.get(c));
+          }
+        }
       }
-      // one barrier per trip: corners of both steps published, both planes read, timeouts agreed on
-      if (__syncthreads_or(bad)) {
-        if (tid == 0 && A.err) atomicExch(A.err, 1);
-        return;
-      }
-      refill(s, pb0);
-      if (two) refill(s + 1, pb1);
-      if (out_row) {
-        if (s >= 1) output(s, cA, own_s);
-        if (two) output(s + 1, cB, ownB);
-      }
+      return true;
+    };
+    // two steps per trip with the sets swapped (the carries stay where they were written)
+    for (int s = 0; s <= zc; s += 2) {
+      if (!step(s, FA, UA, ownA, FB, UB, ownB)) return;
+      if (s + 1 > zc) break;
+      if (!step(s + 1, FB, UB, ownB, FA, UA, ownA)) return;
     }
   } else {
     R F0[4][3], own[3], dummy[3];
-    face_modes<PL>(bufs, ty, tx, n, TY + 2, F0, dummy);
+    face_modes(bufs, ty, tx, n, F0, dummy);
     if (tma) {
       // buffer 0 is free once every thread has read plane 0
       if (__syncthreads_or(bad)) {
         if (tid == 0 && A.err) atomicExch(A.err, 1);
         return;
       }
-      if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0], cs);
+      if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, y0, TY + 2, n, &bars[0]);
     }
     R Up[4][3];
 #pragma unroll
@@ -530,11 +464,11 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
       } else {
         cp_wait_all();
         __syncthreads();
-        if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr, cs);
+        if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, y0, TY + 2, n, tid, nthr);
       }
 
       R F1[4][3], own1[3];
-      face_modes<PL>(cur, ty, tx, n, TY + 2, F1, own1);
+      face_modes(cur, ty, tx, n, F1, own1);
       // element modes: z level
       R Q[8][3];
 #pragma unroll
@@ -579,9 +513,9 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
         // warp 0 refills (its lanes issue the rows in parallel); a block of fewer than 32 threads
         // has no full warp, and thread 0 issues the rows alone
         if (full_warp0) {
-          if (tid < 32) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid, cs);
+          if (tid < 32) tma_plane_warp(cur, in, zr, y0, TY + 2, n, &bars[jb], tid);
         } else if (tid == 0) {
-          tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb], cs);
+          tma_plane(cur, in, zr, y0, TY + 2, n, &bars[jb]);
         }
       }
       if (++jb == NS) { jb = 0; jpar ^= 1u; }
@@ -818,19 +752,18 @@ int launch_stencil(pgj_ctx* c, int mode, int loads, int prec, const void* in, vo
   A.err = c->cond + 2;
   A.rel_flags = rel_flags;
   const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
-  // the FP32 recurrence vectors of a slab-fused context are component-planar, (3, N) per load
+  // the FP32 recurrence vectors of a slab-fused context are component-planar, (3, N) per load: the
+  // operator writes its q that way (p is read interleaved)
   const bool planar = prec == PGJ_FP32 && c->fused && (mode == kPCG || (mode == kPlain && planar_plain));
   // TMA rows need 16-byte aligned starts and sizes: (3 n * element size) % 16 == 0 and an aligned base
-  // (component-planar rows: n * element size, the component blocks 4 n^3 bytes apart)
-  const size_t rowb = (planar ? 1 : 3) * size_t(n) * tsz;
+  const size_t rowb = 3 * size_t(n) * tsz;
   A.tma = (rowb % 16 == 0) && (reinterpret_cast<uintptr_t>(in) % 16 == 0) ? 1 : 0;
   dim3 grid(c->sg.ntiles, c->sg.nchunks, loads), block(n, c->sg.ty + 1);
   A.stages = A.tma ? c->sg.stages : 2;
   // FP32 recurrence operator with FP64 arithmetic (high-contrast mixed solves)
   const bool r64 = prec == PGJ_FP32 && mode == kPCG && c->op64;
   const size_t rsz = r64 ? 8 : tsz;  // corner exchange in the arithmetic type
-  const size_t xslots = rsz == 4 ? 4 : 2;  // FP32 loop: one barrier per two z-steps, four slots
-  const size_t smem = tsz * size_t(A.stages) * (c->sg.ty + 2) * 3 * n + rsz * xslots * 9 * (c->sg.ty + 1) * n +
+  const size_t smem = tsz * size_t(A.stages) * (c->sg.ty + 2) * 3 * n + rsz * 2 * 9 * (c->sg.ty + 1) * n +
                       32 * 4 * 8 + 16 + 8 * A.stages + 64;
   if (c->sg.ntiles * c->sg.nchunks > kMaxPartials) return PGJ_ERR_UNSUPPORTED;
   if (mode != kPlain && mode != kPCG && !(mode == kResidual && prec == PGJ_FP64)) return PGJ_ERR_ARGUMENT;

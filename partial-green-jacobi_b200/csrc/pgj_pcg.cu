@@ -31,11 +31,15 @@ __device__ __forceinline__ void store_chunk(T* __restrict__ dst, const T (&v)[Ch
   for (int i = 0; i < 3; ++i) d[i] = reinterpret_cast<const V*>(v)[i];
 }
 
-template <typename T, typename U>
+// FLEX (FP32 flexible direction update): also r_new . z_prev, where z_prev = s.w - mean(s.w) of the
+// previous Green apply, still held in `sw` (nothing writes it between update_p and this kernel).
+template <typename T, typename U, bool FLEX = false>
 __global__ void __launch_bounds__(256) k_update_ur(int n, U* __restrict__ u, T* __restrict__ r,
                                                    const T* __restrict__ p, const T* __restrict__ q, LoadScalars* scal,
-                                                   double* partials, int cap, double rel_delta2) {
+                                                   double* partials, int cap, double rel_delta2,
+                                                   const T* __restrict__ sw = nullptr) {
   constexpr int CH = Chunk<T>::CH;
+  constexpr int NV = FLEX ? 5 : 4;
   const size_t N = size_t(n) * n * n, N3 = 3 * N;
   const int load = blockIdx.y;
   LoadScalars& S = scal[load];
@@ -43,7 +47,8 @@ __global__ void __launch_bounds__(256) k_update_ur(int n, U* __restrict__ u, T* 
   const double alpha = S.alpha;
   const T a = T(alpha);
   const size_t off = size_t(load) * N3;
-  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  double acc[NV] = {};
+  const T mz[3] = {T(S.mean_z[0]), T(S.mean_z[1]), T(S.mean_z[2])};
   const size_t nch = N3 / CH;
   for (size_t ch = size_t(blockIdx.x) * blockDim.x + threadIdx.x; ch < nch; ch += size_t(gridDim.x) * blockDim.x) {
     const size_t k = off + ch * CH;
@@ -68,18 +73,25 @@ __global__ void __launch_bounds__(256) k_update_ur(int n, U* __restrict__ u, T* 
       acc[0] += rd * rd;
       acc[1 + j % 3] += rd;
     }
+    if constexpr (FLEX) {
+      T zv[CH];
+      load_chunk<T>(sw + k, zv);
+#pragma unroll
+      for (int j = 0; j < CH; ++j) acc[NV - 1] += double(rv[j]) * double(zv[j] - mz[j % 3]);
+    }
     store_chunk<T>(r + k, rv);
   }
-  __shared__ double red[128];
-  block_sum<4>(acc, red);
+  __shared__ double red[32 * NV];
+  block_sum<NV>(acc, red);
   double* part = partials + size_t(load) * kPartialQ * kMaxPartials;
   if (threadIdx.x == 0)
-    for (int k = 0; k < 4; ++k) part[k * kMaxPartials + blockIdx.x] = acc[k];
+    for (int k = 0; k < NV; ++k) part[k * kMaxPartials + blockIdx.x] = acc[k];
   if (!last_block(&S.ticket[kTicketUpdate], gridDim.x)) return;
   if (threadIdx.x < 32) {
-    double v[4];
-    for (int k = 0; k < 4; ++k) v[k] = warp_sum_partials(part + k * kMaxPartials, gridDim.x);
+    double v[5] = {};
+    for (int k = 0; k < NV; ++k) v[k] = warp_sum_partials(part + k * kMaxPartials, gridDim.x);
     if (threadIdx.x == 0) {
+      if constexpr (FLEX) S.rz_cross = v[4];
       const double res2 = v[0];
       const bool finite = isfinite(res2);
       const int it = S.iterations + 1;
@@ -113,7 +125,19 @@ static unsigned update_blocks(const pgj_ctx* c, int prec) {
 int launch_update_ur(pgj_ctx* c, int loads, int prec, double* u64, void* uT, cudaStream_t s) {
   dim3 grid(update_blocks(c, prec), loads);
   const double rel = c->rel_delta2;
-  if (prec == PGJ_FP32) {
+  if (prec == PGJ_FP32 && c->flex) {
+    const float* sw = static_cast<const float*>(c->sw);
+    if (u64)
+      k_update_ur<float, double, true><<<grid, 256, 0, s>>>(c->n, u64, static_cast<float*>(c->r),
+                                                            static_cast<const float*>(c->p),
+                                                            static_cast<const float*>(c->q), c->scal, c->partials,
+                                                            c->cap, rel, sw);
+    else
+      k_update_ur<float, float, true><<<grid, 256, 0, s>>>(c->n, static_cast<float*>(uT), static_cast<float*>(c->r),
+                                                           static_cast<const float*>(c->p),
+                                                           static_cast<const float*>(c->q), c->scal, c->partials,
+                                                           c->cap, rel, sw);
+  } else if (prec == PGJ_FP32) {
     if (u64)
       k_update_ur<float, double><<<grid, 256, 0, s>>>(c->n, u64, static_cast<float*>(c->r),
                                                       static_cast<const float*>(c->p), static_cast<const float*>(c->q),

@@ -109,8 +109,9 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   double* red = reinterpret_cast<double*>(b1 + size_t(n) * nsp);
   const size_t N = size_t(nn) * n, N3 = 3 * N;
   const size_t node0 = size_t(z) * nn;
-  // FP32 recurrence vectors are component-planar, (3, N) per load: the slab's values are contiguous;
-  // FP64 vectors (and the FP64 true residual) keep the node-major interleaved layout
+  // FP32 recurrence vectors r, d and q are component-planar, (3, N) per load: the slab's values are
+  // contiguous; the direction p (the operator's input, staged by rows) and the FP64 vectors (the FP64
+  // true residual included) keep the node-major interleaved layout
   constexpr bool PL = sizeof(T) == 4;
   constexpr int KS = PL ? 1 : 3;                           // element stride of consecutive nodes
   const size_t off = PL ? size_t(load) * N3 + size_t(c) * N + node0
@@ -127,7 +128,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   const T a = T(alpha);
   // nodes whose loads are in flight together (the FP64 update keeps five doubles per node)
   constexpr int UNR = (MODE == kSlabUpdate && sizeof(T) == 8) ? 2 : 4;
-  const T* pg = reinterpret_cast<const T*>(A.p) + off;
+  const T* pg = reinterpret_cast<const T*>(A.p) + off64;  // interleaved: stride 3
   const T* qg = reinterpret_cast<const T*>(A.q) + off;
   const T* zg = FLEX ? reinterpret_cast<const T*>(A.zprev) + off : nullptr;
   U* ug = reinterpret_cast<U*>(A.u) + off;
@@ -143,7 +144,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
       if (i < nn) {
         const size_t k = size_t(KS) * i;
         sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[3 * size_t(i)];
-        if (MODE == kSlabUpdate) { pv[j] = pg[k]; qv[j] = qg[k]; rv[j] = r[k]; uv[j] = ug[k]; }
+        if (MODE == kSlabUpdate) { pv[j] = pg[3 * size_t(i)]; qv[j] = qg[k]; rv[j] = r[k]; uv[j] = ug[k]; }
         else if (MODE == kSlabSync) rv[j] = T(r64[3 * size_t(i)]);
         else rv[j] = r[k];
       }
@@ -396,11 +397,11 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
   }
   const T* wv = real_view<T>(res2);
   const size_t node0 = size_t(z) * nn;
-  constexpr bool PL = sizeof(T) == 4;  // FP32 recurrence vectors are component-planar
+  constexpr bool PL = sizeof(T) == 4;  // FP32 recurrence vectors other than p are component-planar
   constexpr int KS = PL ? 1 : 3;
   const size_t N = size_t(nn) * n;
   const size_t off = PL ? size_t(load) * 3 * N + size_t(c) * N + node0 : size_t(load) * 3 * N + 3 * node0 + c;
-  T* p = reinterpret_cast<T*>(A.p) + off;
+  T* p = reinterpret_cast<T*>(A.p) + (size_t(load) * 3 * N + 3 * node0 + c);  // interleaved: stride 3
   const size_t dsg = size_t(load / A.lpd) * 3 * size_t(nn) * n;  // this load's design
   const double* sc = A.scale + dsg + 3 * node0 + c;
   const float* s32 = sizeof(T) == 4 ? A.scale32 + dsg + size_t(c) * nn * n + node0 : nullptr;  // coalesced
@@ -415,7 +416,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
       const int i = i0 + j * nthr;
       if (i < nn) {
         sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[3 * size_t(i)];
-        pv[j] = A.init ? T(0) : p[size_t(KS) * i];
+        pv[j] = A.init ? T(0) : p[3 * size_t(i)];
       }
     }
 #pragma unroll
@@ -425,7 +426,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_ifxy(const SlabA
         const int y = fdiv(i, A.div_n), x = i - y * n;
         const T w = wv[2 * ((y >> 1) * lpx + x) + (y & 1)];
         const T zv = T(sv[j]) * w - m;
-        p[size_t(KS) * i] = A.init ? zv : zv + beta * pv[j];
+        p[3 * size_t(i)] = A.init ? zv : zv + beta * pv[j];
         if constexpr (FLEX) reinterpret_cast<T*>(A.zprev)[off + size_t(KS) * i] = zv;
       }
     }

@@ -617,16 +617,20 @@ def test_serving_eta_alpha_runs_high_contrast_lineages_mixed(pkg):
     assert rel(res[0].C, ref[0].C) < 1e-7
 
 
-@pytest.mark.parametrize("n,emin,alpha", [(16, 1e-6, 0.5), (32, 1e-9, 0.8125), (64, 1e-6, 0.5)])
-def test_mixed_flexible_beta_certifies_and_agrees(pkg, n, emin, alpha):
-    """The flexible (Polak-Ribiere) direction update of the FP32 recurrences certifies to 1e-8 and
-    gives C_H within the mixed tolerance of the FP64 solve; FP64 contexts refuse it."""
+@pytest.mark.parametrize("n,emin,alpha,fused", [(16, 1e-6, 0.5, True), (32, 1e-9, 0.8125, True), (64, 1e-6, 0.5, True),
+                                                (16, 1e-6, 0.5, False), (24, 1e-9, 0.5, False)])
+def test_mixed_flexible_beta_certifies_and_agrees(pkg, n, emin, alpha, fused):
+    """The flexible (Polak-Ribiere) direction update of the FP32 recurrences, in the slab-fused and
+    in the step-by-step iteration, certifies to 1e-8 and gives C_H within the mixed tolerance of the
+    FP64 solve; FP64 contexts refuse it."""
     lam, mu = pkg.PAPER_MEDIUM
     a = dev(pkg.baseline_design(n, 2, emin))
     out = {}
     for prec, flex in (("fp64", False), ("mixed", True)):
         op = pkg.Operator(n, 6, lam, mu, precision=prec)
         if flex:
+            op.set_fused_iteration(fused)
+            assert op.fused_iteration == fused
             op.set_flexible_beta(True)
         op.set_material(a)
         op.set_alpha(alpha)
