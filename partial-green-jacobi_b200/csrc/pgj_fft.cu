@@ -671,6 +671,7 @@ static GreenArgs green_args(pgj_ctx* c, int prec, const void* r) {
   A.sw = c->sw; A.scal = c->scal; A.partials = c->partials;
   A.axis = axis_table(c);
   A.lam = c->lam; A.mu = c->mu;
+  A.flex = prec == PGJ_FP32 ? c->flex : 0;  // beta of the FP32 recurrence: flexible form when set
   return A;
 }
 
@@ -700,7 +701,6 @@ int launch_fz_fused(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s) 
   A.finalize_fz = 1;
   A.fused = 1;
   A.shat = c->shat;
-  A.flex = prec == PGJ_FP32 ? c->flex : 0;
   const char* e = std::getenv("PGJ_FZ64");
   if (c->n == 64 && !(e && e[0] == '0'))  // line transforms in registers (PGJ_FZ64=0: generic pass)
     return prec == PGJ_FP32 ? run_fz64<float>(c, loads, A, s) : run_fz64<double>(c, loads, A, s);
