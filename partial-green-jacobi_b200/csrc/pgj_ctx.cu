@@ -94,6 +94,8 @@ static Layout make_layout(int n, int D, int lpd, int prec) {
   y.spec = take(2 * tsz * 3 * size_t(n) * n * nsp * L);
   y.shat = take(2 * tsz * 3 * size_t(n) * n * nsp * D);
   y.scale32 = take(prec == PGJ_FP32 ? sizeof(float) * N3 * D : 0);
+  // boundary rows of the halo-free FP32 operator: n planes x n / ty tiles x 3n per load, ty >= 2
+  y.qb = take(prec == PGJ_FP32 && slab_fits_shape(n, prec) ? sizeof(float) * (N3 / 2 + 3 * size_t(n)) * L : 0);
   y.total = o;
   return y;
 }
@@ -115,7 +117,7 @@ static int capture_cert(pgj_ctx* c, int L, cudaStream_t s) {
 static int capture_iteration(pgj_ctx* c, int L, cudaStream_t s, cudaGraphConditionalHandle h, bool last) {
   const int prec = c->prec;
   int st;
-  if ((st = launch_stencil(c, kPCG, L, prec, c->p, c->q, nullptr, nullptr, s))) return st;
+  if ((st = launch_recurrence_operator(c, L, prec, s))) return st;
   if (c->fused) {
     // u += alpha p, r -= alpha q and the x/y transforms of s.r; z pass; inverse x/y and p update
     if ((st = launch_fxy(c, L, prec, kSlabUpdateL, prec == PGJ_FP32 ? c->d : static_cast<void*>(c->x), s))) return st;
@@ -208,7 +210,7 @@ static int capture_into(cudaGraph_t body, F&& fn) {
 static int capture_iteration_rel(pgj_ctx* c, int L, cudaStream_t s, cudaGraphConditionalHandle hw) {
   int st;
   const bool fused = c->fused != 0;
-  if ((st = launch_stencil(c, kPCG, L, PGJ_FP32, c->p, c->q, nullptr, nullptr, s))) return st;
+  if ((st = launch_recurrence_operator(c, L, PGJ_FP32, s))) return st;
   if (fused) st = launch_fxy(c, L, PGJ_FP32, kSlabUpdateL, c->d, s);
   else st = launch_update_ur(c, L, PGJ_FP32, nullptr, c->d, s);
   if (st) return st;
@@ -449,6 +451,12 @@ int pgj_ctx_create_batch(int n, int designs, int loads, int precision, double la
   c->x = reinterpret_cast<double*>(b + y.x);
   c->r64 = precision == PGJ_FP32 ? reinterpret_cast<double*>(b + y.r64) : nullptr;
   c->r = b + y.r; c->p = b + y.p; c->q = b + y.q; c->sw = b + y.sw; c->spec = b + y.spec;
+  c->qb = precision == PGJ_FP32 && slab_fits_shape(n, precision) ? static_cast<void*>(b + y.qb) : nullptr;
+  c->hg = hf_geom(n, loads);
+  {
+    const char* e = std::getenv("PGJ_HF");
+    c->hf = c->qb != nullptr && !(e && e[0] == '0') ? 1 : 0;
+  }
   c->shat = b + y.shat;
   c->scale32 = precision == PGJ_FP32 ? reinterpret_cast<float*>(b + y.scale32) : nullptr;
   c->partials = reinterpret_cast<double*>(b + y.partials);
@@ -857,7 +865,7 @@ int pgj_profile_iteration(pgj_ctx* c, int loads, const double* macros, int reps,
   for (int k = 0; k < 2 * PGJ_PROFILE_KERNELS; ++k) cudaEventCreate(&ev[k]);
   double acc[PGJ_PROFILE_KERNELS] = {0};
   auto launch_k = [&](int k) -> int {
-    if (k == 0) return launch_stencil(c, kPCG, loads, prec, c->p, c->q, nullptr, nullptr, s);
+    if (k == 0) return launch_recurrence_operator(c, loads, prec, s);
     if (fused && k == 1) return launch_fxy(c, loads, prec, kSlabUpdateL, u, s);
     if (fused && k == 2) return launch_fz_fused(c, loads, prec, false, s);
     if (fused && k == 3) return launch_ifxy(c, loads, prec, false, s, 0, false);

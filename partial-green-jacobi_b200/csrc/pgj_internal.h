@@ -59,6 +59,7 @@ struct StencilArgs {
   int tma;                     // stage planes with bulk async copies (aligned rows) instead of cp.async
   int stages;                  // plane buffers in the staging pipeline
   int* err;                    // set to 1 if a bounded device wait expired
+  void* qb;                    // halo-free recurrence operator: boundary rows (L, n, ntiles, 3, n)
 };
 
 // Partial-sum slots per load per kernel (blocks per load upper bound).
@@ -72,7 +73,7 @@ constexpr int kAuxDoubles = kAuxPartials + kMaxPartials;
 
 struct Layout {
   size_t a, scale, scale32, symbol, symbol32, tw, solutions, f, x, r, p, q, sw, spec, shat, partials, scal, macros,
-      cond, r64, d, aux, total;
+      cond, r64, d, aux, qb, total;
 };
 
 struct Graphs;
@@ -106,6 +107,9 @@ struct pgj_ctx {
   void* r;             // (L, 3N) T
   void* p;             // (L, 3N) T
   void* q;             // (L, 3N) T
+  void* qb;            // FP32 slab-fused contexts: (L, n, n / hg.ty, 3, n) boundary rows of the halo-free operator
+  pgj::StencilGeom hg; // halo-free recurrence operator geometry (FP32 slab-fused contexts)
+  int hf;              // FP32 slab-fused recurrences use the halo-free operator (PGJ_HF=0: the halo form)
   void* sw;            // (L, 3N) T  s . w (unprojected preconditioned residual)
   void* spec;          // (L, 3, n, n, nsp) complex T
   void* shat;          // (D, 3, n, n, nsp) complex T: DFT of each component of the scale field
@@ -168,6 +172,14 @@ int launch_scale32(pgj_ctx* c, cudaStream_t s);
 // slab-fused iteration (pgj_slab.cu)
 enum SlabLaunch { kSlabUpdateL = 0, kSlabInitL = 1, kSlabSyncL = 2 };
 bool slab_fits(const pgj_ctx* c);
+bool slab_fits_shape(int n, int prec);
+// halo-free FP32 recurrence operator (pgj_operator.cu): geometry, launch, and whether a context's
+// recurrence uses it (FP32, slab-fused, FP32 arithmetic, not switched off)
+StencilGeom hf_geom(int n, int lpd);
+int launch_stencil_hf(pgj_ctx* c, int loads, cudaStream_t s);
+inline bool uses_hf(const pgj_ctx* c, int prec) { return prec == PGJ_FP32 && c->fused && c->hf && !c->op64; }
+// the recurrence operator q = K p (and alpha = r.z / p.q) of one PCG iteration
+int launch_recurrence_operator(pgj_ctx* c, int loads, int prec, cudaStream_t s);
 int prepare_slab_kernels();
 int launch_fxy(pgj_ctx* c, int loads, int prec, int mode, void* u, cudaStream_t s);
 int launch_ifxy(pgj_ctx* c, int loads, int prec, bool init, cudaStream_t s, cudaGraphConditionalHandle h,

@@ -588,6 +588,285 @@ __global__ void __launch_bounds__(OCC == 1 ? 512 : 256, OCC) k_stencil(const Ste
   }
 }
 
+// ------------------------------------------------------------------ halo-free recurrence operator
+// The FP32 recurrence operator of slab-fused mixed contexts, without the halo element row of
+// k_stencil: a block owns TY node rows (TY divides n) and exactly the TY element rows whose lower
+// node row is one of them, so no element is computed twice. Thread (x, ty) owns element (x, y0 + ty).
+// A node row y0 + ty, ty >= 1, gets all four corner contributions inside the block (same order as
+// k_stencil) and is stored. The first row y0 of a tile gets its own elements' corners here; those of
+// the element row below the tile are the upper corners of the top element row of the tile below, which
+// that block writes, per z-plane and tile, to the boundary array qb ([load][z][tile][component][x]);
+// the slab update (k_fxy) adds qb to q on the rows y % TY == 0 as it reads q. (Adding the two parts
+// atomically onto zeroed rows of q instead measured slower: the atomics cost the operator 4.6 us and
+// re-zeroing the rows cost the slab update 4 us.) p^T q counts each part in the block that computes
+// it, with p of the node it belongs to (the upper face of the top row), so alpha = r.z / p^T q is the
+// quantity of the halo form; only the rounding of the first rows differs.
+// Planes are staged as TY + 1 node rows (y0 .. y0 + TY), q is written component-planar, p is read
+// interleaved.
+__device__ __forceinline__ void face_modes_top(const float* buf, int row, int x, int n, Tri<float> (&F)[4],
+                                               Tri<float>& own, Tri<float>& top) {
+  const int xp = (x + 1 == n) ? 0 : x + 1;
+  const float* r0 = buf + row * 3 * n;
+  const float* r1 = r0 + 3 * n;
+  const Tri<float> u00 = Tri<float>::load(r0 + 3 * x), u10 = Tri<float>::load(r0 + 3 * xp);
+  const Tri<float> u01 = Tri<float>::load(r1 + 3 * x), u11 = Tri<float>::load(r1 + 3 * xp);
+  own = u00;
+  top = u01;
+  const Tri<float> sx0 = u10 + u00, dx0 = u10 - u00, sx1 = u11 + u01, dx1 = u11 - u01;
+  F[0] = sx1 + sx0;
+  F[1] = dx1 + dx0;
+  F[2] = sx1 - sx0;
+  F[3] = dx1 - dx0;
+}
+
+__global__ void __launch_bounds__(256, 2) k_stencil_hf(const StencilArgs A) {
+  using T = float;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int n = A.n, TY = A.ty;
+  const int tx = threadIdx.x, ty = threadIdx.y;
+  const int tid = tx + n * ty, nthr = n * TY;
+  const int load = blockIdx.z;
+  const int ntiles = gridDim.x;
+  const int nblk = gridDim.x * gridDim.y, blk = blockIdx.x + gridDim.x * blockIdx.y;
+  const size_t N = size_t(n) * n * n;
+  const int y0 = blockIdx.x * TY, z0 = blockIdx.y * A.zc;
+  const int zc = min(A.zc, n - z0);
+  const int ey = y0 + ty;  // element row = own node row (< n: TY divides n)
+  LoadScalars& S = A.scal[load];
+  if (S.active == 0) return;
+  T* out = reinterpret_cast<T*>(A.out) + size_t(load) * 3 * N;
+  // boundary rows for the tile above (the first row of tile blockIdx.x + 1, periodic in y)
+  T* qb = reinterpret_cast<T*>(A.qb) + size_t(load) * n * ntiles * 3 * n +
+          size_t(blockIdx.x + 1 == ntiles ? 0 : blockIdx.x + 1) * 3 * n + tx;
+  const T* in = reinterpret_cast<const T*>(A.in) + size_t(load) * 3 * N;
+
+  const int NS = A.tma ? A.stages : 2;
+  const int rows = TY + 1;
+  const int planevals = rows * 3 * n;
+  const int nt = n * TY;
+  T* bufs = reinterpret_cast<T*>(smem_raw);
+  T* xch = bufs + NS * planevals;  // [parity][corner 10 / 01 / 11][thread][3]
+  const int xsz = 3 * nt * 3;
+  double* red = reinterpret_cast<double*>(xch + 2 * xsz + 2);
+  red = reinterpret_cast<double*>((reinterpret_cast<uintptr_t>(red) + 15) & ~uintptr_t(15));
+  uint64_t* bars = reinterpret_cast<uint64_t*>(red + 32 * 4);
+  const bool tma = A.tma != 0;
+  const int nplanes = zc + 2;
+  // the staging helpers take rows (y0' - 1 + r) mod n: y0' = y0 + 1 gives rows y0 .. y0 + TY
+  const int ys = y0 + 1;
+
+  bool bad = false;
+  if (tma) {
+    if (tid == 0) {
+      for (int b = 0; b < NS; ++b) mbar_init(&bars[b], 1);
+      fence_mbar_init();
+    }
+    __syncthreads();
+    if (tid == 0)
+      for (int j = 0; j < NS && j < nplanes; ++j)
+        tma_plane(bufs + j * planevals, in, (z0 - 1 + j + n) % n, ys, rows, n, &bars[j]);
+    bad = !mbar_wait(&bars[0], 0);
+  } else {
+    stage_plane(bufs, in, (z0 - 1 + n) % n, ys, rows, n, tid, nthr);
+    stage_plane(bufs + planevals, in, z0 % n, ys, rows, n, tid, nthr);
+    cp_wait_one();
+    __syncthreads();
+  }
+  double acc = 0.0;
+  Tri<T> FA[4], UA[4], ownA, topA, FB[4], UB[4], ownB, topB;
+  face_modes_top(bufs, ty, tx, n, FA, ownB, topB);
+  if (tma) {
+    if (__syncthreads_or(bad)) {
+      if (tid == 0 && A.err) atomicExch(A.err, 1);
+      return;
+    }
+    if (tid == 0 && NS < nplanes) tma_plane(bufs, in, (z0 - 1 + NS) % n, ys, rows, n, &bars[0]);
+  }
+#pragma unroll
+  for (int f = 0; f < 4; ++f) UA[f] = Tri<T>::make(T(0), T(0), T(0));
+  ownA = Tri<T>::make(T(0), T(0), T(0));
+  topA = ownA;
+
+  const double* arow = A.a + size_t(load / A.lpd) * N + size_t(ey) * n + tx;
+  const size_t aplane = size_t(n) * n;
+  int za = (z0 - 1 + n) % n;
+  double a_next = __ldg(arow + size_t(za) * aplane);
+  int jb = 1 % NS;
+  unsigned jpar = 0u;
+  int zr = (z0 + NS) % n;
+  const bool full_warp0 = nthr >= 32;
+  const int txl = tx == 0 ? n - 1 : tx - 1;
+  const int tl = ty * n + txl;                       // element to the left (periodic x)
+  const int tb = (ty >= 1 ? ty - 1 : 0) * n + tx;    // element below (inside the tile)
+  const int tbl = (ty >= 1 ? ty - 1 : 0) * n + txl;
+  const int tme = ty * n + tx;
+  const bool top_row = ty == TY - 1;
+
+  auto step = [&](int s, const Tri<T> (&F0)[4], const Tri<T> (&Up)[4], const Tri<T>& own0, const Tri<T>& top0,
+                  Tri<T> (&F1)[4], Tri<T> (&U)[4], Tri<T>& own1, Tri<T>& top1) -> bool {
+    const int ez = z0 - 1 + s;
+    const T ae = T(a_next);
+    if (s < zc) {
+      za = za + 1 == n ? 0 : za + 1;
+      a_next = __ldg(arow + size_t(za) * aplane);
+    }
+    T* cur = bufs + jb * planevals;
+    if (tma) {
+      bad = bad || !mbar_wait(&bars[jb], jpar);
+    } else {
+      cp_wait_all();
+      __syncthreads();
+      if (s < zc) stage_plane(((s & 1) ? bufs + planevals : bufs), in, (z0 + s + 1) % n, ys, rows, n, tid, nthr);
+    }
+    face_modes_top(cur, ty, tx, n, F1, own1, top1);
+    T Q[8][3];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      const Tri<T> sum = F1[f] + F0[f], dif = F1[f] - F0[f];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) { Q[f][c] = sum.get(c); Q[f + 4][c] = dif.get(c); }
+    }
+    T P[8][3];
+    element_modal<T>(Q, ae, A.kc, P);
+    Tri<T> G[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      const Tri<T> lo = Tri<T>::make(P[f][0], P[f][1], P[f][2]);
+      const Tri<T> hi = Tri<T>::make(P[f + 4][0], P[f + 4][1], P[f + 4][2]);
+      U[f] = lo + hi;
+      G[f] = (lo - hi) + Up[f];
+    }
+    Tri<T> c00, c01;
+    T* xb = xch + (s & 1) * xsz;
+    if (s >= 1) {
+      const Tri<T> ly0 = G[0] - G[2], ly1 = G[1] - G[3];
+      const Tri<T> uy0 = G[0] + G[2], uy1 = G[1] + G[3];
+      c00 = ly0 - ly1;
+      c01 = uy0 - uy1;
+      (ly0 + ly1).store(xb + (0 * nt + tme) * 3);
+      c01.store(xb + (1 * nt + tme) * 3);
+      (uy0 + uy1).store(xb + (2 * nt + tme) * 3);
+    }
+    if (__syncthreads_or(bad)) {
+      if (tid == 0 && A.err) atomicExch(A.err, 1);
+      return false;
+    }
+    if (tma && s + 1 + NS < nplanes) {
+      if (full_warp0) {
+        if (tid < 32) tma_plane_warp(cur, in, zr, ys, rows, n, &bars[jb], tid);
+      } else if (tid == 0) {
+        tma_plane(cur, in, zr, ys, rows, n, &bars[jb]);
+      }
+    }
+    if (++jb == NS) { jb = 0; jpar ^= 1u; }
+    zr = zr + 1 == n ? 0 : zr + 1;
+    if (s >= 1) {
+      Tri<T> qx = c00 + Tri<T>::load(xb + (0 * nt + tl) * 3);
+      if (ty >= 1) qx = (qx + Tri<T>::load(xb + (1 * nt + tb) * 3)) + Tri<T>::load(xb + (2 * nt + tbl) * 3);
+      const size_t node = (size_t(ez) * n + ey) * n + tx;
+      T* o = out + node;
+      o[0] = qx.get(0); o[N] = qx.get(1); o[2 * N] = qx.get(2);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) acc += double(own0.get(c)) * double(qx.get(c));
+      if (top_row) {
+        // node (x, y0 + TY) of plane ez: this element's (x, y+1) corner and the left element's (x+1, y+1)
+        const Tri<T> bq = c01 + Tri<T>::load(xb + (2 * nt + tl) * 3);
+        T* b = qb + size_t(ez) * ntiles * 3 * n;
+        b[0] = bq.get(0); b[n] = bq.get(1); b[2 * n] = bq.get(2);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc += double(top0.get(c)) * double(bq.get(c));
+      }
+    }
+    return true;
+  };
+  for (int s = 0; s <= zc; s += 2) {
+    if (!step(s, FA, UA, ownA, topA, FB, UB, ownB, topB)) return;
+    if (s + 1 > zc) break;
+    if (!step(s + 1, FB, UB, ownB, topB, FA, UA, ownA, topA)) return;
+  }
+
+  double v1[1] = {acc};
+  block_sum<1>(v1, red);
+  double* part = A.partials + size_t(load) * kPartialQ * kMaxPartials;
+  if (tid == 0) part[blk] = v1[0];
+  if (!last_block(&S.ticket[kTicketApply], nblk)) return;
+  if (tid < 32) {
+    const double den = warp_sum_partials(part, nblk);
+    if (tid == 0) {
+      const double rz = S.rz;
+      const bool valid = isfinite(den) && den > 0.0 && isfinite(rz) && rz > 0.0;
+      S.failed = valid ? 0 : 1;
+      S.alpha = valid ? rz / den : 0.0;
+    }
+  }
+}
+
+// Halo-free geometry for grid edge n and `lpd` loads per design: TY the largest divisor of n with
+// n TY <= 256 threads (TY >= 2), and the z chunking that fills the launch's block slots best
+// (blocks per design over whole waves of 148 SMs times the blocks per SM, times the share of element
+// planes that are not recomputed at chunk starts). Depends on n and lpd only, so a design's
+// decomposition (and summation order) is the same alone and in a batch. PGJ_HF_TY / PGJ_HF_ZC pin it.
+StencilGeom hf_geom(int n, int lpd) {
+  StencilGeom g;
+  g.ty = 2;
+  for (int t = 2; t <= n && n * t <= 256; ++t)
+    if (n % t == 0) g.ty = t;
+  if (const char* e = std::getenv("PGJ_HF_TY")) {
+    const int v = std::atoi(e);
+    if (v >= 2 && v <= n && n % v == 0 && n * v <= 256) g.ty = v;
+  }
+  g.ntiles = n / g.ty;
+  const int threads = n * g.ty;
+  int bps = 65536 / (threads * 128);
+  bps = bps < 1 ? 1 : (bps > 8 ? 8 : bps);
+  const int slots = 148 * bps;
+  double best = -1.0;
+  int best_zc = n;
+  for (int nch = 1; nch <= (n / 4 > 1 ? n / 4 : 1); ++nch) {
+    const int zc = (n + nch - 1) / nch;
+    const int chunks = (n + zc - 1) / zc;
+    const long blocks = long(lpd) * g.ntiles * chunks;
+    const long waves = (blocks + slots - 1) / slots;
+    const double eff = double(blocks) / double(waves * slots) * double(zc) / double(zc + 1);
+    if (eff > best + 1e-9) { best = eff; best_zc = zc; }
+  }
+  g.zc = best_zc;
+  if (const char* e = std::getenv("PGJ_HF_ZC")) {
+    const int v = std::atoi(e);
+    if (v >= 1 && v <= n) g.zc = v;
+  }
+  g.nchunks = (n + g.zc - 1) / g.zc;
+  g.stages = 2;
+  g.occ = 1;
+  return g;
+}
+
+int launch_recurrence_operator(pgj_ctx* c, int loads, int prec, cudaStream_t s) {
+  if (uses_hf(c, prec)) return launch_stencil_hf(c, loads, s);
+  return launch_stencil(c, kPCG, loads, prec, c->p, c->q, nullptr, nullptr, s);
+}
+
+int launch_stencil_hf(pgj_ctx* c, int loads, cudaStream_t s) {
+  const int n = c->n;
+  const StencilGeom& g = c->hg;
+  StencilArgs A;
+  A.n = n; A.ty = g.ty; A.zc = g.zc;
+  A.lpd = c->lpd;
+  A.a = c->a; A.in = c->p; A.out = c->q; A.f = nullptr; A.active_ext = nullptr;
+  A.scal = c->scal; A.partials = c->partials; A.kc = c->kc; A.iteration_cap = c->cap;
+  A.err = c->cond + 2;
+  A.rel_flags = nullptr;
+  A.qb = c->qb;
+  const size_t rowb = 3 * size_t(n) * sizeof(float);
+  A.tma = (rowb % 16 == 0) && (reinterpret_cast<uintptr_t>(c->p) % 16 == 0) ? 1 : 0;
+  A.stages = A.tma ? g.stages : 2;
+  if (g.ntiles * g.nchunks > kMaxPartials || n * g.ty > 256) return PGJ_ERR_UNSUPPORTED;
+  const size_t smem = sizeof(float) * size_t(A.stages) * (g.ty + 1) * 3 * n + sizeof(float) * 2 * 9 * g.ty * n +
+                      32 * 4 * 8 + 16 + 8 * A.stages + 64;
+  k_stencil_hf<<<dim3(g.ntiles, g.nchunks, loads), dim3(n, g.ty), smem, s>>>(A);
+  return check_launch();
+}
+
 // Tile table: shapes per (grid edge, precision) picked offline by the project's tuner
 // (partial-green-jacobi_b200/tune_tiles.py, which times every candidate on a B200 and writes
 // pgj_tiles.inc). Contexts of a tabulated size take these shapes without timing anything, so the
@@ -721,6 +1000,7 @@ static void set_stencil_smem(int lim) {
 int prepare_stencil_kernels() {
   set_stencil_smem<1>(220 * 1024);  // below the 227 KB opt-in less the static shared memory
   set_stencil_smem<3>(72 * 1024);
+  cudaFuncSetAttribute(k_stencil_hf, cudaFuncAttributeMaxDynamicSharedMemorySize, 110 * 1024);
   return check_launch();
 }
 

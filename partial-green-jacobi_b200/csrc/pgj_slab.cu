@@ -50,6 +50,10 @@ struct SlabArgs {
   int set_cond;           // ifxy: set the WHILE condition (any load active, bounded body count)
   cudaGraphConditionalHandle h;
   int* counters;
+  const void* qb;         // halo-free operator: boundary rows (L, n, hf_ntiles, 3, n), added to q
+  int hf_ty, hf_ntiles;   // its tile height (rows y % hf_ty == 0 take a boundary row) and tile count
+  int hf_shift;           // log2 of the tile height when it is a power of 2, else -1
+  FastDiv div_hfty;
 };
 
 // the loop body runs at most cap + 100 times per attempt (the same bound as the unfused loop body)
@@ -94,7 +98,9 @@ __device__ __forceinline__ void line64(cplx<T> (&v)[8], cplx<T>* L, int t, const
 // the n x nsp half-spectrum rows.
 // FLEX: the flexible direction update (FP32 only) adds r_new . z_prev to the block sums; a separate
 // instantiation, so the plain forms keep their register budget (the runtime branch cost 3-6 us).
-template <typename T, typename U, int MODE, bool W4, bool R64, bool FLEX = false>
+// HFQ (FP32 update mode): q comes from the halo-free operator, whose first rows of every tile
+// (y % hf_ty == 0) lack the contributions of the element row below; those are in qb and added here.
+template <typename T, typename U, int MODE, bool W4, bool R64, bool FLEX = false, bool HFQ = false>
 __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabArgs A) {
   using C = cplx<T>;
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -133,9 +139,13 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   const T* zg = FLEX ? reinterpret_cast<const T*>(A.zprev) + off : nullptr;
   U* ug = reinterpret_cast<U*>(A.u) + off;
   const double* r64 = A.r64 + off64;
+  // the slab's boundary rows, read per node (staging them in shared memory first, behind a block
+  // barrier, measured slower: 52.7 vs 50.0 us)
+  const T* qbb = HFQ ? reinterpret_cast<const T*>(A.qb) + ((size_t(load) * n + z) * A.hf_ntiles * 3 + c) * size_t(n)
+                     : nullptr;
   for (int i0 = tid; i0 < nn; i0 += UNR * nthr) {
     // all loads of UNR nodes first, then the updates and stores
-    T pv[UNR], qv[UNR], rv[UNR];
+    T pv[UNR], qv[UNR], rv[UNR], bv[UNR];
     U uv[UNR];
     double sv[UNR];
 #pragma unroll
@@ -145,6 +155,20 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
         const size_t k = size_t(KS) * i;
         sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[3 * size_t(i)];
         if (MODE == kSlabUpdate) { pv[j] = pg[3 * size_t(i)]; qv[j] = qg[k]; rv[j] = r[k]; uv[j] = ug[k]; }
+        if constexpr (HFQ) {
+          // row and tile of node i without divisions where n (64) and the tile height are powers of 2
+          int yy, xx, t;
+          bool first;
+          if (R64) { yy = i >> 6; xx = i & 63; } else { yy = fdiv(i, A.div_n); xx = i - yy * n; }
+          if (A.hf_shift >= 0) {
+            t = yy >> A.hf_shift;
+            first = (yy & ((1 << A.hf_shift) - 1)) == 0;
+          } else {
+            t = fdiv(yy, A.div_hfty);
+            first = t * A.hf_ty == yy;
+          }
+          bv[j] = first ? qbb[t * 3 * n + xx] : T(0);
+        }
         else if (MODE == kSlabSync) rv[j] = T(r64[3 * size_t(i)]);
         else rv[j] = r[k];
       }
@@ -158,7 +182,7 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
         T rj = rv[j];
         if (MODE == kSlabUpdate) {
           ug[k] = uv[j] + U(alpha) * U(pv[j]);
-          rj = rj - a * qv[j];
+          rj = rj - a * (HFQ ? qv[j] + bv[j] : qv[j]);
           r[k] = rj;
           const double rd = double(rj);
           acc[0] += rd * rd;
@@ -449,15 +473,20 @@ static int slab_threads(const pgj_ctx* c) {
   return t;
 }
 
-bool slab_fits(const pgj_ctx* c) {
-  const size_t tsz = c->prec == PGJ_FP32 ? 4 : 8;
-  const int nsp = c->ns + (c->ns & 1);
-  return slab_smem(c->n, nsp, tsz) <= 110 * 1024;  // two blocks per SM
+bool slab_fits_shape(int n, int prec) {
+  const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
+  const int ns = n / 2 + 1, nsp = ns + (ns & 1);
+  return slab_smem(n, nsp, tsz) <= 110 * 1024;  // two blocks per SM
 }
+
+bool slab_fits(const pgj_ctx* c) { return slab_fits_shape(c->n, c->prec); }
 
 template <typename T, typename U, bool W4, bool R64, bool FLEX = false>
 static void set_fxy_smem(int lim) {
   cudaFuncSetAttribute(k_fxy<T, U, kSlabUpdate, W4, R64, FLEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+  if (sizeof(T) == 4)
+    cudaFuncSetAttribute(k_fxy<T, U, kSlabUpdate, W4, R64, FLEX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         lim);
   cudaFuncSetAttribute(k_fxy<T, U, kSlabInit, W4, R64, FLEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_fxy<T, U, kSlabSync, W4, R64, FLEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
   cudaFuncSetAttribute(k_ifxy<T, W4, R64, FLEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
@@ -512,7 +541,10 @@ static SlabArgs slab_args(pgj_ctx* c, int loads, int prec) {
 template <typename T, typename U, bool W4, bool R64, bool FLEX = false>
 static void fxy_kernel(int mode, dim3 grid, int thr, size_t smem, cudaStream_t s, const SlabArgs& A) {
   switch (mode) {
-    case kSlabUpdate: k_fxy<T, U, kSlabUpdate, W4, R64, FLEX><<<grid, thr, smem, s>>>(A); break;
+    case kSlabUpdate:
+      if (sizeof(T) == 4 && A.qb) k_fxy<T, U, kSlabUpdate, W4, R64, FLEX, sizeof(T) == 4><<<grid, thr, smem, s>>>(A);
+      else k_fxy<T, U, kSlabUpdate, W4, R64, FLEX><<<grid, thr, smem, s>>>(A);
+      break;
     case kSlabInit: k_fxy<T, U, kSlabInit, W4, R64, FLEX><<<grid, thr, smem, s>>>(A); break;
     default: k_fxy<T, U, kSlabSync, W4, R64, FLEX><<<grid, thr, smem, s>>>(A); break;
   }
@@ -521,6 +553,15 @@ static void fxy_kernel(int mode, dim3 grid, int thr, size_t smem, cudaStream_t s
 int launch_fxy(pgj_ctx* c, int loads, int prec, int mode, void* u, cudaStream_t s) {
   SlabArgs A = slab_args(c, loads, prec);
   A.u = u;
+  if (mode == kSlabUpdate && uses_hf(c, prec)) {  // q from the halo-free operator: add its boundary rows
+    A.qb = c->qb;
+    A.hf_ty = c->hg.ty;
+    A.hf_ntiles = c->hg.ntiles;
+    A.div_hfty = make_fastdiv(unsigned(c->hg.ty));
+    A.hf_shift = -1;
+    for (int b = 0; b < 8; ++b)
+      if ((1 << b) == c->hg.ty) A.hf_shift = b;
+  }
   const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
   const dim3 grid(3, c->n, loads);
   const int thr = slab_threads(c);

@@ -652,3 +652,48 @@ def test_mixed_flexible_beta_certifies_and_agrees(pkg, n, emin, alpha, fused):
             assert its[("mixed", True, False)] != its[("mixed", False, False)], its
     with pytest.raises(RuntimeError, match="unsupported"):
         pkg.Operator(8, 6, lam, mu).set_flexible_beta(True)
+
+
+@pytest.mark.parametrize("n,emin,designs", [(16, 1e-6, 1), (48, 1e-9, 1), (64, 1e-6, 2)])
+def test_halo_free_operator_matches_halo_form(pkg, monkeypatch, n, emin, designs):
+    """The halo-free FP32 recurrence operator (each element once, first tile rows added atomically
+    onto zero) against the halo form (PGJ_HF=0): both certify, C_H agrees within the mixed tolerance
+    and the iteration counts within 2% (only the rounding of the first tile rows differs); the
+    halo-free results are bitwise reproducible, alone and in a batched context."""
+    lam, mu = pkg.PAPER_MEDIUM
+    a = [pkg.baseline_design(n, 30 + d, emin) for d in range(designs)]
+    out = {}
+    for hf in ("1", "0", "1"):
+        monkeypatch.setenv("PGJ_HF", hf)
+        res = []
+        for d in range(designs):
+            op = pkg.Operator(n, 6, lam, mu, precision="mixed")
+            op.set_material(dev(a[d]))
+            op.set_alpha(0.8125 if emin < 1e-8 else 0.5)
+            u = torch.zeros((6, 3 * n ** 3), dtype=torch.float64, device="cuda")
+            infos, st = op.solve(np.eye(6), 1e-8, u)
+            assert st == 0 and all(i["relative_residual"] <= 1e-8 for i in infos), (hf, infos)
+            res.append((op.effective_tensor(u).cpu().numpy(), [i["iterations"] for i in infos]))
+        out.setdefault(hf, []).append(res)
+    (hf1, hf1b), (halo,) = out["1"], out["0"]
+    for d in range(designs):
+        assert np.array_equal(hf1[d][0], hf1b[d][0]) and hf1[d][1] == hf1b[d][1]
+        assert rel(hf1[d][0], halo[d][0]) < 1e-7
+        for x, y in zip(hf1[d][1], halo[d][1]):
+            assert abs(x - y) <= max(2, 0.02 * y), (hf1[d][1], halo[d][1])
+    if designs > 1:
+        monkeypatch.setenv("PGJ_HF", "1")
+        bop = pkg.BatchedOperator(n, designs, 6, lam, mu, "mixed")
+        s = torch.cuda.current_stream()
+        for d in range(designs):
+            bop.set_material(d, dev(a[d]), s)
+            bop.set_alpha(d, 0.8125 if emin < 1e-8 else 0.5, s)
+        u = torch.zeros((designs * 6, 3 * n ** 3), dtype=torch.float64, device="cuda")
+        bop.solve_async(designs, np.eye(6), 1e-8, u, s)
+        infos, st = bop.wait(designs, s)
+        assert st == 0
+        for d in range(designs):
+            C = torch.empty((6, 6), dtype=torch.float64, device="cuda")
+            bop.effective_tensor(d, u[6 * d:6 * (d + 1)], C, s)
+            assert np.array_equal(C.cpu().numpy(), hf1[d][0])
+            assert [i["iterations"] for i in infos[6 * d:6 * (d + 1)]] == hf1[d][1]
