@@ -19,6 +19,7 @@
 #include "pgj_fft_engine.cuh"
 #include <cstdlib>
 #include <cstring>
+#include <type_traits>
 
 namespace pgj {
 
@@ -139,50 +140,59 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   const T* zg = FLEX ? reinterpret_cast<const T*>(A.zprev) + off : nullptr;
   U* ug = reinterpret_cast<U*>(A.u) + off;
   const double* r64 = A.r64 + off64;
-  // the slab's boundary rows, read per node (staging them in shared memory first, behind a block
-  // barrier, measured slower: 52.7 vs 50.0 us)
+  // The halo-free operator leaves the first row of every tile (y % hf_ty == 0) without the
+  // contributions of the element row below; those are in qb. With HFQ the update runs in two passes:
+  // the other rows first (a cheap row test per node), then the first rows with q + qb (reading qb
+  // per node in one pass measured 7 us slower, staging it in shared memory behind a barrier 9 us).
   const T* qbb = HFQ ? reinterpret_cast<const T*>(A.qb) + ((size_t(load) * n + z) * A.hf_ntiles * 3 + c) * size_t(n)
                      : nullptr;
-  for (int i0 = tid; i0 < nn; i0 += UNR * nthr) {
-    // all loads of UNR nodes first, then the updates and stores
-    T pv[UNR], qv[UNR], rv[UNR], bv[UNR];
-    U uv[UNR];
-    double sv[UNR];
+  const int hshift = HFQ ? A.hf_shift : 0;
+  auto first_row = [&](int i) -> bool {
+    if constexpr (!HFQ) return false;
+    const int yy = R64 ? (i >> 6) : fdiv(i, A.div_n);
+    if (hshift >= 0) return (yy & ((1 << hshift) - 1)) == 0;
+    return fdiv(yy, A.div_hfty) * A.hf_ty == yy;
+  };
+  // count nodes, node index i = idx(e), BND: the first rows (q + qb)
+  auto pass = [&](int count, auto idx, auto bnd_tag) {
+    constexpr bool BND = decltype(bnd_tag)::value;
+    for (int e0 = tid; e0 < count; e0 += UNR * nthr) {
+      // all loads of UNR nodes first, then the updates and stores
+      T pv[UNR], qv[UNR], rv[UNR];
+      U uv[UNR];
+      double sv[UNR];
+      bool on[UNR];
 #pragma unroll
-    for (int j = 0; j < UNR; ++j) {
-      const int i = i0 + j * nthr;
-      if (i < nn) {
+      for (int j = 0; j < UNR; ++j) {
+        const int e = e0 + j * nthr;
+        on[j] = e < count;
+        if (!on[j]) continue;
+        const int i = idx(e);
+        if (!BND && first_row(i)) { on[j] = false; continue; }
         const size_t k = size_t(KS) * i;
         sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[3 * size_t(i)];
-        if (MODE == kSlabUpdate) { pv[j] = pg[3 * size_t(i)]; qv[j] = qg[k]; rv[j] = r[k]; uv[j] = ug[k]; }
-        if constexpr (HFQ) {
-          // row and tile of node i without divisions where n (64) and the tile height are powers of 2
-          int yy, xx, t;
-          bool first;
-          if (R64) { yy = i >> 6; xx = i & 63; } else { yy = fdiv(i, A.div_n); xx = i - yy * n; }
-          if (A.hf_shift >= 0) {
-            t = yy >> A.hf_shift;
-            first = (yy & ((1 << A.hf_shift) - 1)) == 0;
-          } else {
-            t = fdiv(yy, A.div_hfty);
-            first = t * A.hf_ty == yy;
+        if (MODE == kSlabUpdate) {
+          pv[j] = pg[3 * size_t(i)]; qv[j] = qg[k]; rv[j] = r[k]; uv[j] = ug[k];
+          if constexpr (BND) {
+            const int t = R64 ? (i >> (6 + hshift)) : fdiv(fdiv(i, A.div_n), A.div_hfty);
+            qv[j] += qbb[t * 3 * n + (i - t * A.hf_ty * n)];
           }
-          bv[j] = first ? qbb[t * 3 * n + xx] : T(0);
+        } else if (MODE == kSlabSync) {
+          rv[j] = T(r64[3 * size_t(i)]);
+        } else {
+          rv[j] = r[k];
         }
-        else if (MODE == kSlabSync) rv[j] = T(r64[3 * size_t(i)]);
-        else rv[j] = r[k];
       }
-    }
 #pragma unroll
-    for (int j = 0; j < UNR; ++j) {
-      const int i = i0 + j * nthr;
-      if (i < nn) {
+      for (int j = 0; j < UNR; ++j) {
+        if (!on[j]) continue;
+        const int i = idx(e0 + j * nthr);
         const size_t k = size_t(KS) * i;
         const int y = fdiv(i, A.div_n), x = i - y * n;
         T rj = rv[j];
         if (MODE == kSlabUpdate) {
           ug[k] = uv[j] + U(alpha) * U(pv[j]);
-          rj = rj - a * (HFQ ? qv[j] + bv[j] : qv[j]);
+          rj = rj - a * qv[j];
           r[k] = rj;
           const double rd = double(rj);
           acc[0] += rd * rd;
@@ -195,6 +205,14 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
         packed[2 * ((y >> 1) * lpx + x) + (y & 1)] = T(sv[j]) * rj;
       }
     }
+  };
+  pass(nn, [](int e) { return e; }, std::false_type{});
+  if constexpr (HFQ) {
+    // the first rows: e = (tile, x) -> node (tile * hf_ty, x)
+    pass(A.hf_ntiles * n, [&](int e) {
+      const int t = R64 ? (e >> 6) : fdiv(e, A.div_n);
+      return t * A.hf_ty * n + (e - t * n);
+    }, std::true_type{});
   }
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
