@@ -95,7 +95,7 @@ static Layout make_layout(int n, int D, int lpd, int prec) {
   y.shat = take(2 * tsz * 3 * size_t(n) * n * nsp * D);
   y.scale32 = take(prec == PGJ_FP32 ? sizeof(float) * N3 * D : 0);
   // boundary rows of the halo-free FP32 operator: n planes x n / ty tiles x 3n per load, ty >= 2
-  y.qb = take(prec == PGJ_FP32 && slab_fits_shape(n, prec) ? sizeof(float) * (N3 / 2 + 3 * size_t(n)) * L : 0);
+  y.qb = take(prec == PGJ_FP32 && n == 64 ? sizeof(float) * (N3 / 2 + 3 * size_t(n)) * L : 0);
   y.total = o;
   return y;
 }
@@ -451,9 +451,12 @@ int pgj_ctx_create_batch(int n, int designs, int loads, int precision, double la
   c->x = reinterpret_cast<double*>(b + y.x);
   c->r64 = precision == PGJ_FP32 ? reinterpret_cast<double*>(b + y.r64) : nullptr;
   c->r = b + y.r; c->p = b + y.p; c->q = b + y.q; c->sw = b + y.sw; c->spec = b + y.spec;
-  c->qb = precision == PGJ_FP32 && slab_fits_shape(n, precision) ? static_cast<void*>(b + y.qb) : nullptr;
+  c->qb = precision == PGJ_FP32 && n == 64 ? static_cast<void*>(b + y.qb) : nullptr;
   c->hg = hf_geom(n, loads);
   {
+    // the halo-free operator pays off where the slab update's first-row pass is cheap: the n = 64
+    // register-transform path (row tests by shifts); measured per size, every other grid was slower
+    // per iteration with it (n = 16: 51.7 vs 47.6 us, 54: 263 vs 247, 96: 687 vs 683)
     const char* e = std::getenv("PGJ_HF");
     c->hf = c->qb != nullptr && !(e && e[0] == '0') ? 1 : 0;
   }

@@ -107,7 +107,7 @@ struct pgj_ctx {
   void* r;             // (L, 3N) T
   void* p;             // (L, 3N) T
   void* q;             // (L, 3N) T
-  void* qb;            // FP32 slab-fused contexts: (L, n, n / hg.ty, 3, n) boundary rows of the halo-free operator
+  void* qb;            // FP32 contexts at n = 64: (L, n, n / hg.ty, 3, n) boundary rows of the halo-free operator
   pgj::StencilGeom hg; // halo-free recurrence operator geometry (FP32 slab-fused contexts)
   int hf;              // FP32 slab-fused recurrences use the halo-free operator (PGJ_HF=0: the halo form)
   void* sw;            // (L, 3N) T  s . w (unprojected preconditioned residual)
@@ -177,7 +177,10 @@ bool slab_fits_shape(int n, int prec);
 // recurrence uses it (FP32, slab-fused, FP32 arithmetic, not switched off)
 StencilGeom hf_geom(int n, int lpd);
 int launch_stencil_hf(pgj_ctx* c, int loads, cudaStream_t s);
-inline bool uses_hf(const pgj_ctx* c, int prec) { return prec == PGJ_FP32 && c->fused && c->hf && !c->op64; }
+bool slab_register_path(const pgj_ctx* c, int prec);  // the n = 64 register-transform slab kernels
+inline bool uses_hf(const pgj_ctx* c, int prec) {
+  return prec == PGJ_FP32 && c->fused && c->hf && !c->op64 && slab_register_path(c, prec);
+}
 // the recurrence operator q = K p (and alpha = r.z / p.q) of one PCG iteration
 int launch_recurrence_operator(pgj_ctx* c, int loads, int prec, cudaStream_t s);
 int prepare_slab_kernels();

@@ -51,10 +51,10 @@ struct SlabArgs {
   int set_cond;           // ifxy: set the WHILE condition (any load active, bounded body count)
   cudaGraphConditionalHandle h;
   int* counters;
-  const void* qb;         // halo-free operator: boundary rows (L, n, hf_ntiles, 3, n), added to q
-  int hf_ty, hf_ntiles;   // its tile height (rows y % hf_ty == 0 take a boundary row) and tile count
-  int hf_shift;           // log2 of the tile height when it is a power of 2, else -1
-  FastDiv div_hfty;
+  // The halo-free operator's boundary rows reach the update (k_fxy, update mode) through fields the
+  // update does not use otherwise: r64 (the sync mode's FP64 residual) carries qb, (L, n, ntiles, 3, n),
+  // init the tile height and set_cond the tile count. Four more fields in this parameter block (which
+  // the kernels copy to local memory) had made the generic FP32 update twice as slow at n = 48.
 };
 
 // the loop body runs at most cap + 100 times per attempt (the same bound as the unfused loop body)
@@ -144,75 +144,117 @@ __global__ void __launch_bounds__(W4 ? 288 : 512, W4 ? 4 : 2) k_fxy(const SlabAr
   // contributions of the element row below; those are in qb. With HFQ the update runs in two passes:
   // the other rows first (a cheap row test per node), then the first rows with q + qb (reading qb
   // per node in one pass measured 7 us slower, staging it in shared memory behind a barrier 9 us).
-  const T* qbb = HFQ ? reinterpret_cast<const T*>(A.qb) + ((size_t(load) * n + z) * A.hf_ntiles * 3 + c) * size_t(n)
-                     : nullptr;
-  const int hshift = HFQ ? A.hf_shift : 0;
-  auto first_row = [&](int i) -> bool {
-    if constexpr (!HFQ) return false;
-    const int yy = R64 ? (i >> 6) : fdiv(i, A.div_n);
-    if (hshift >= 0) return (yy & ((1 << hshift) - 1)) == 0;
-    return fdiv(yy, A.div_hfty) * A.hf_ty == yy;
-  };
-  // count nodes, node index i = idx(e), BND: the first rows (q + qb)
-  auto pass = [&](int count, auto idx, auto bnd_tag) {
-    constexpr bool BND = decltype(bnd_tag)::value;
-    for (int e0 = tid; e0 < count; e0 += UNR * nthr) {
+  if constexpr (HFQ) {
+    // the lambdas live only in this branch: capturing the update's locals by reference elsewhere put
+    // them in local memory and doubled the generic slab update (n = 48: 78.8 vs 40.0 us)
+    const int hf_ty = A.init, hf_ntiles = A.set_cond;
+    const T* qbb = reinterpret_cast<const T*>(A.r64) + ((size_t(load) * n + z) * hf_ntiles * 3 + c) * size_t(n);
+    const int hshift = (hf_ty & (hf_ty - 1)) == 0 ? __ffs(hf_ty) - 1 : -1;
+    auto first_row = [&](int i) -> bool {
+      if constexpr (!HFQ) return false;
+      const int yy = R64 ? (i >> 6) : fdiv(i, A.div_n);
+      if (hshift >= 0) return (yy & ((1 << hshift) - 1)) == 0;
+      return (yy / hf_ty) * hf_ty == yy;
+    };
+    // count nodes, node index i = idx(e), BND: the first rows (q + qb)
+    auto pass = [&](int count, auto idx, auto bnd_tag) {
+      constexpr bool BND = decltype(bnd_tag)::value;
+      for (int e0 = tid; e0 < count; e0 += UNR * nthr) {
+        // all loads of UNR nodes first, then the updates and stores
+        T pv[UNR], qv[UNR], rv[UNR];
+        U uv[UNR];
+        double sv[UNR];
+        bool on[UNR];
+  #pragma unroll
+        for (int j = 0; j < UNR; ++j) {
+          const int e = e0 + j * nthr;
+          on[j] = e < count;
+          if (!on[j]) continue;
+          const int i = idx(e);
+          if (!BND && first_row(i)) { on[j] = false; continue; }
+          const size_t k = size_t(KS) * i;
+          sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[3 * size_t(i)];
+          if (MODE == kSlabUpdate) {
+            pv[j] = pg[3 * size_t(i)]; qv[j] = qg[k]; rv[j] = r[k]; uv[j] = ug[k];
+            if constexpr (BND) {
+              const int t = R64 ? (i >> (6 + hshift)) : fdiv(i, A.div_n) / hf_ty;
+              qv[j] += qbb[t * 3 * n + (i - t * hf_ty * n)];
+            }
+          } else if (MODE == kSlabSync) {
+            rv[j] = T(r64[3 * size_t(i)]);
+          } else {
+            rv[j] = r[k];
+          }
+        }
+  #pragma unroll
+        for (int j = 0; j < UNR; ++j) {
+          if (!on[j]) continue;
+          const int i = idx(e0 + j * nthr);
+          const size_t k = size_t(KS) * i;
+          const int y = fdiv(i, A.div_n), x = i - y * n;
+          T rj = rv[j];
+          if (MODE == kSlabUpdate) {
+            ug[k] = uv[j] + U(alpha) * U(pv[j]);
+            rj = rj - a * qv[j];
+            r[k] = rj;
+            const double rd = double(rj);
+            acc[0] += rd * rd;
+            acc[1] += rd;
+            if constexpr (FLEX) acc[FLEX ? 2 : 0] += rd * double(zg[k]);
+          } else if (MODE == kSlabSync) {
+            r[k] = rj;
+          }
+          // rows 2l and 2l+1 packed as the real and imaginary parts of complex line l
+          packed[2 * ((y >> 1) * lpx + x) + (y & 1)] = T(sv[j]) * rj;
+        }
+      }
+    };
+    pass(nn, [](int e) { return e; }, std::false_type{});
+    // the first rows: e = (tile, x) -> node (tile * hf_ty, x)
+    pass(hf_ntiles * n, [&](int e) {
+      const int t = R64 ? (e >> 6) : fdiv(e, A.div_n);
+      return t * hf_ty * n + (e - t * n);
+    }, std::true_type{});
+  } else {
+    for (int i0 = tid; i0 < nn; i0 += UNR * nthr) {
       // all loads of UNR nodes first, then the updates and stores
       T pv[UNR], qv[UNR], rv[UNR];
       U uv[UNR];
       double sv[UNR];
-      bool on[UNR];
 #pragma unroll
       for (int j = 0; j < UNR; ++j) {
-        const int e = e0 + j * nthr;
-        on[j] = e < count;
-        if (!on[j]) continue;
-        const int i = idx(e);
-        if (!BND && first_row(i)) { on[j] = false; continue; }
-        const size_t k = size_t(KS) * i;
-        sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[3 * size_t(i)];
-        if (MODE == kSlabUpdate) {
-          pv[j] = pg[3 * size_t(i)]; qv[j] = qg[k]; rv[j] = r[k]; uv[j] = ug[k];
-          if constexpr (BND) {
-            const int t = R64 ? (i >> (6 + hshift)) : fdiv(fdiv(i, A.div_n), A.div_hfty);
-            qv[j] += qbb[t * 3 * n + (i - t * A.hf_ty * n)];
-          }
-        } else if (MODE == kSlabSync) {
-          rv[j] = T(r64[3 * size_t(i)]);
-        } else {
-          rv[j] = r[k];
+        const int i = i0 + j * nthr;
+        if (i < nn) {
+          const size_t k = size_t(KS) * i;
+          sv[j] = sizeof(T) == 4 ? double(s32[i]) : sc[3 * size_t(i)];
+          if (MODE == kSlabUpdate) { pv[j] = pg[3 * size_t(i)]; qv[j] = qg[k]; rv[j] = r[k]; uv[j] = ug[k]; }
+          else if (MODE == kSlabSync) rv[j] = T(r64[3 * size_t(i)]);
+          else rv[j] = r[k];
         }
       }
 #pragma unroll
       for (int j = 0; j < UNR; ++j) {
-        if (!on[j]) continue;
-        const int i = idx(e0 + j * nthr);
-        const size_t k = size_t(KS) * i;
-        const int y = fdiv(i, A.div_n), x = i - y * n;
-        T rj = rv[j];
-        if (MODE == kSlabUpdate) {
-          ug[k] = uv[j] + U(alpha) * U(pv[j]);
-          rj = rj - a * qv[j];
-          r[k] = rj;
-          const double rd = double(rj);
-          acc[0] += rd * rd;
-          acc[1] += rd;
-          if constexpr (FLEX) acc[FLEX ? 2 : 0] += rd * double(zg[k]);
-        } else if (MODE == kSlabSync) {
-          r[k] = rj;
+        const int i = i0 + j * nthr;
+        if (i < nn) {
+          const size_t k = size_t(KS) * i;
+          const int y = fdiv(i, A.div_n), x = i - y * n;
+          T rj = rv[j];
+          if (MODE == kSlabUpdate) {
+            ug[k] = uv[j] + U(alpha) * U(pv[j]);
+            rj = rj - a * qv[j];
+            r[k] = rj;
+            const double rd = double(rj);
+            acc[0] += rd * rd;
+            acc[1] += rd;
+            if constexpr (FLEX) acc[FLEX ? 2 : 0] += rd * double(zg[k]);
+          } else if (MODE == kSlabSync) {
+            r[k] = rj;
+          }
+          // rows 2l and 2l+1 packed as the real and imaginary parts of complex line l
+          packed[2 * ((y >> 1) * lpx + x) + (y & 1)] = T(sv[j]) * rj;
         }
-        // rows 2l and 2l+1 packed as the real and imaginary parts of complex line l
-        packed[2 * ((y >> 1) * lpx + x) + (y & 1)] = T(sv[j]) * rj;
       }
     }
-  };
-  pass(nn, [](int e) { return e; }, std::false_type{});
-  if constexpr (HFQ) {
-    // the first rows: e = (tile, x) -> node (tile * hf_ty, x)
-    pass(A.hf_ntiles * n, [&](int e) {
-      const int t = R64 ? (e >> 6) : fdiv(e, A.div_n);
-      return t * A.hf_ty * n + (e - t * n);
-    }, std::true_type{});
   }
   __syncthreads();
   const C* tw = reinterpret_cast<const C*>(A.tw);
@@ -502,7 +544,7 @@ bool slab_fits(const pgj_ctx* c) { return slab_fits_shape(c->n, c->prec); }
 template <typename T, typename U, bool W4, bool R64, bool FLEX = false>
 static void set_fxy_smem(int lim) {
   cudaFuncSetAttribute(k_fxy<T, U, kSlabUpdate, W4, R64, FLEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-  if (sizeof(T) == 4)
+  if constexpr (sizeof(T) == 4 && R64)
     cudaFuncSetAttribute(k_fxy<T, U, kSlabUpdate, W4, R64, FLEX, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          lim);
   cudaFuncSetAttribute(k_fxy<T, U, kSlabInit, W4, R64, FLEX>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
@@ -536,6 +578,8 @@ static bool slab_r64(const pgj_ctx* c, int prec, int thr) {
   return c->n == 64 && thr == 288 && !(e && e[0] == '0');
 }
 
+bool slab_register_path(const pgj_ctx* c, int prec) { return slab_r64(c, prec, slab_threads(c)); }
+
 static SlabArgs slab_args(pgj_ctx* c, int loads, int prec) {
   SlabArgs A;
   std::memset(&A, 0, sizeof(A));
@@ -560,8 +604,16 @@ template <typename T, typename U, bool W4, bool R64, bool FLEX = false>
 static void fxy_kernel(int mode, dim3 grid, int thr, size_t smem, cudaStream_t s, const SlabArgs& A) {
   switch (mode) {
     case kSlabUpdate:
-      if (sizeof(T) == 4 && A.qb) k_fxy<T, U, kSlabUpdate, W4, R64, FLEX, sizeof(T) == 4><<<grid, thr, smem, s>>>(A);
-      else k_fxy<T, U, kSlabUpdate, W4, R64, FLEX><<<grid, thr, smem, s>>>(A);
+      // the halo-free operator's consumer exists for the n = 64 register path only: compiled for the
+      // generic paths as well, its instantiations made their plain update twice as slow (n = 48: 75.8
+      // vs 39.9 us), though that code is not run there
+      if constexpr (sizeof(T) == 4 && R64) {
+        if (A.init) {
+          k_fxy<T, U, kSlabUpdate, W4, R64, FLEX, true><<<grid, thr, smem, s>>>(A);
+          break;
+        }
+      }
+      k_fxy<T, U, kSlabUpdate, W4, R64, FLEX><<<grid, thr, smem, s>>>(A);
       break;
     case kSlabInit: k_fxy<T, U, kSlabInit, W4, R64, FLEX><<<grid, thr, smem, s>>>(A); break;
     default: k_fxy<T, U, kSlabSync, W4, R64, FLEX><<<grid, thr, smem, s>>>(A); break;
@@ -572,13 +624,9 @@ int launch_fxy(pgj_ctx* c, int loads, int prec, int mode, void* u, cudaStream_t 
   SlabArgs A = slab_args(c, loads, prec);
   A.u = u;
   if (mode == kSlabUpdate && uses_hf(c, prec)) {  // q from the halo-free operator: add its boundary rows
-    A.qb = c->qb;
-    A.hf_ty = c->hg.ty;
-    A.hf_ntiles = c->hg.ntiles;
-    A.div_hfty = make_fastdiv(unsigned(c->hg.ty));
-    A.hf_shift = -1;
-    for (int b = 0; b < 8; ++b)
-      if ((1 << b) == c->hg.ty) A.hf_shift = b;
+    A.r64 = static_cast<const double*>(c->qb);  // the update mode's unused fields (see SlabArgs)
+    A.init = c->hg.ty;
+    A.set_cond = c->hg.ntiles;
   }
   const size_t tsz = prec == PGJ_FP32 ? 4 : 8;
   const dim3 grid(3, c->n, loads);
