@@ -180,8 +180,12 @@ __device__ __forceinline__ void stage_lines(const cplx<T>* __restrict__ src, cpl
 
 // All stages over `nl` lines, ping-pong between b0 and b1 with one block barrier per stage; returns
 // the buffer holding the result. `ldiv` divides by nl (LFAST only).
+// Always inlined into the slab kernels, its only callers: as a called function it kept their
+// registers and the plan in local memory across the call (a 440-byte stack frame) and made their
+// speed depend on how many kernels called it (slab update n = 32: 16.5 vs 24.5 us). The per-line
+// fft_line of the unfused passes stays a compiler choice (forced inline it made the z pass slower).
 template <typename T, bool LFAST>
-__device__ cplx<T>* fft_lines(cplx<T>* b0, cplx<T>* b1, int nl, int lp, int es, const FFTPlan& pl,
+__device__ __forceinline__ cplx<T>* fft_lines(cplx<T>* b0, cplx<T>* b1, int nl, int lp, int es, const FFTPlan& pl,
                               const FastDiv& ldiv, const cplx<T>* tw, bool inv, int tid, int nthr) {
   cplx<T>* src = b0;
   cplx<T>* dst = b1;
