@@ -28,10 +28,18 @@ namespace pgj {
 bool make_fft_plan(int n, FFTPlan* plan) {
   plan->n = n;
   plan->nst = 0;
-  int m = n;
-  while (m % 8 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 8; m /= 8; }
-  while (m % 4 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 4; m /= 4; }
-  while (m % 2 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 2; m /= 2; }
+  // powers of two as radix-8 stages, except that 2^(3k+1) takes 8^(k-1) * 4 * 4 rather than 8^k * 2
+  // (a radix-2 stage has n/2 butterflies per line and sizes the block for itself while the radix-8
+  // stage leaves most threads idle: n = 48 as 8 * 2 * 3 vs 4 * 4 * 3)
+  int m = n, e = 0;
+  while (m % 2 == 0) { m /= 2; ++e; }
+  int n8 = e / 3, n4 = e % 3 == 2 ? 1 : 0, n2 = 0;
+  if (e % 3 == 1) {
+    if (n8 >= 1) { n8 -= 1; n4 = 2; } else { n2 = 1; }
+  }
+  for (int i = 0; i < n8 && plan->nst < kMaxStages; ++i) plan->radix[plan->nst++] = 8;
+  for (int i = 0; i < n4 && plan->nst < kMaxStages; ++i) plan->radix[plan->nst++] = 4;
+  for (int i = 0; i < n2 && plan->nst < kMaxStages; ++i) plan->radix[plan->nst++] = 2;
   while (m % 3 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 3; m /= 3; }
   while (m % 5 == 0 && plan->nst < kMaxStages) { plan->radix[plan->nst++] = 5; m /= 5; }
   int ns = 1;
