@@ -31,7 +31,7 @@ extern "C" {
 #define PGJ_ERR_UNSUPPORTED 2    /* grid size outside the built FFT radices / limits */
 #define PGJ_ERR_LAUNCH 3         /* CUDA launch or runtime error (C10_CUDA_KERNEL_LAUNCH_CHECK) */
 #define PGJ_ERR_NONFINITE 4      /* non-finite input or non-positive curvature latch */
-#define PGJ_ERR_ITERATION_CAP 5  /* a recurrence reached the 4000-iteration cap uncertified */
+#define PGJ_ERR_ITERATION_CAP 5  /* the PCG loop ran into its body bound (iteration cap + 100) */
 #define PGJ_ERR_CERTIFICATION 6  /* 'true residual certification failed' (resident.py:208) */
 #define PGJ_ERR_TIMEOUT 7        /* a bounded device wait expired */
 #define PGJ_ERR_WORKSPACE 8      /* workspace missing, too small or misaligned */
