@@ -229,8 +229,8 @@ int pgj_effective_tensor(pgj_ctx* ctx, const double* u, double* C, void* stream)
  * 0.69 MB per GPU, held until exit, and the unit Voigt strains in a statically initialised device
  * table. Accepts 2 <= n <= 256 (PGJ_ERR_ARGUMENT otherwise). The first call on a device (and the
  * first after its context is replaced, e.g. by cudaDeviceReset) looks up the array's device
- * address, so make that first call before any stream capture. All calls share the array: calls that
- * overlap on the GPU race and must be ordered on one stream. */
+ * address. All calls share the array: calls that overlap on the GPU race and must be ordered on one
+ * stream. */
 int pgj_effective_tensor_noalloc(int n, double lam, double mu, const double* a, const double* u, double* C,
                                  void* stream);
 
