@@ -17,19 +17,64 @@
 
 namespace pgj {
 
-__global__ void k_cone(int n, const int32_t* __restrict__ off, const double* __restrict__ w, int count,
-                       const double* __restrict__ x, double* __restrict__ y, const double* flag) {
+// Clipped cone filter y(p) = sum_j w_j x(p + d_j) over the taps whose neighbour lies inside the grid
+// (no periodic wrap). A block covers 32 x 8 columns of the (x, y) plane (x fastest, one warp per
+// row) in one z plane (and every gridDim.z-th plane after it); the tap table is staged in shared
+// memory (dx, dy, dz, the neighbour's linear offset and the weight), kConeChunk taps at a time, so
+// every thread reads a tap as a broadcast. Taps are summed in table order with one fused
+// multiply-add each, the order of the reference's loop, so the result does not depend on the
+// tiling. `flag` (the OC bisection record) ends the launch once the bisection has stopped.
+constexpr int kConeChunk = 512;
+constexpr int kConeX = 32, kConeY = 8;
+struct ConeTap {
+  int dx, dy, dz, pad;
+  long long lin;  // (dz n + dy) n + dx
+  double w;
+};
+
+__global__ void __launch_bounds__(kConeX * kConeY) k_cone_filter(int n, const int32_t* __restrict__ offsets,
+                                                                 const double* __restrict__ weights, int count,
+                                                                 const double* __restrict__ x,
+                                                                 double* __restrict__ y, const double* flag) {
   if (flag && flag[2] == 0.0) return;
-  const size_t N = size_t(n) * n * n;
-  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < N; i += size_t(gridDim.x) * blockDim.x) {
-    const int xx = int(i % n), yy = int((i / n) % n), zz = int(i / (size_t(n) * n));
-    double sum = 0.0;
-    for (int j = 0; j < count; ++j) {
-      const int xj = xx + off[3 * j], yj = yy + off[3 * j + 1], zj = zz + off[3 * j + 2];
-      if (xj >= 0 && xj < n && yj >= 0 && yj < n && zj >= 0 && zj < n)
-        sum += w[j] * x[(size_t(zj) * n + yj) * n + xj];
+  __shared__ ConeTap taps[kConeChunk];
+  const int tid = threadIdx.y * kConeX + threadIdx.x;
+  const int cx = blockIdx.x * kConeX + threadIdx.x, cy = blockIdx.y * kConeY + threadIdx.y;
+  const bool inside = cx < n && cy < n;
+  const unsigned un = unsigned(n);
+  auto stage = [&](int first, int m) {
+    for (int j = tid; j < m; j += kConeX * kConeY) {
+      ConeTap t;
+      t.dx = offsets[3 * (first + j)];
+      t.dy = offsets[3 * (first + j) + 1];
+      t.dz = offsets[3 * (first + j) + 2];
+      t.pad = 0;
+      t.lin = (static_cast<long long>(t.dz) * n + t.dy) * n + t.dx;
+      t.w = weights[first + j];
+      taps[j] = t;
     }
-    y[i] = sum;
+  };
+  const bool resident = count <= kConeChunk;  // the whole table stays staged across the z planes
+  if (resident) stage(0, count);
+  __syncthreads();
+  for (int cz = blockIdx.z; cz < n; cz += gridDim.z) {
+    const size_t at = (size_t(cz) * n + cy) * n + cx;
+    double sum = 0.0;
+    for (int first = 0; first < count; first += kConeChunk) {
+      const int m = min(kConeChunk, count - first);
+      if (!resident) {
+        __syncthreads();  // the previous chunk has been read by every thread
+        stage(first, m);
+        __syncthreads();
+      }
+      if (!inside) continue;
+      for (int j = 0; j < m; ++j) {
+        const ConeTap& t = taps[j];
+        if (unsigned(cx + t.dx) < un && unsigned(cy + t.dy) < un && unsigned(cz + t.dz) < un)
+          sum += t.w * x[static_cast<long long>(at) + t.lin];
+      }
+    }
+    if (inside) y[at] = sum;
   }
 }
 
@@ -221,6 +266,15 @@ using namespace pgj;
 
 namespace {
 constexpr int kOCBlocks = 296;
+// cone filter launch: one block per 32 x 8 column tile and z plane (n = 64: 1024 blocks, up to
+// seven resident per SM). Splitting the planes over about kOCBlocks blocks, each walking three or
+// four of them, measured 61.5 against 34.8 us at n = 64 (93 taps)
+dim3 cone_grid(int n) {
+  const int bx = (n + kConeX - 1) / kConeX, by = (n + kConeY - 1) / kConeY;
+  const int bz = std::min(n, 65535);  // the kernel walks the planes beyond the grid's z limit
+  return dim3(unsigned(bx), unsigned(by), unsigned(bz));
+}
+const dim3 kConeBlock(kConeX, kConeY);
 // scratch layout for the OC chains: 4 fields of N doubles, then 8 doubles of bisection state,
 // an int ticket and kOCBlocks partials.
 struct OCScratch {
@@ -242,7 +296,8 @@ extern "C" {
 int pgj_cone_filter(int n, const int32_t* offsets, const double* weights, int count, const double* x, double* y,
                     void* stream) {
   if (n < 2 || !offsets || !weights || count < 1 || !x || !y) return PGJ_ERR_ARGUMENT;
-  k_cone<<<kOCBlocks, 256, 0, static_cast<cudaStream_t>(stream)>>>(n, offsets, weights, count, x, y, nullptr);
+  k_cone_filter<<<cone_grid(n), kConeBlock, 0, static_cast<cudaStream_t>(stream)>>>(n, offsets, weights, count, x, y,
+                                                                                   nullptr);
   return check_launch();
 }
 
@@ -269,14 +324,14 @@ int pgj_paper_oc(int n, const int32_t* offsets, const double* weights, int count
   if (e != cudaSuccess) return set_cuda_error(e);
   // g -> f0 (then ratio), dv -> f1
   k_paper_sens_in<<<kOCBlocks, 256, 0, s>>>(N, ph, dp, hs, energy, emin, w.f2, w.f3);
-  k_cone<<<kOCBlocks, 256, 0, s>>>(n, offsets, weights, count, w.f2, w.f0, nullptr);
-  k_cone<<<kOCBlocks, 256, 0, s>>>(n, offsets, weights, count, w.f3, w.f1, nullptr);
+  k_cone_filter<<<cone_grid(n), kConeBlock, 0, s>>>(n, offsets, weights, count, w.f2, w.f0, nullptr);
+  k_cone_filter<<<cone_grid(n), kConeBlock, 0, s>>>(n, offsets, weights, count, w.f3, w.f1, nullptr);
   k_paper_ratio<<<kOCBlocks, 256, 0, s>>>(N, w.f0, w.f1, w.bounds);
   int st = check_launch();
   if (st) return st;
   for (int it = 0; it < 180; ++it) {
     k_paper_candidate<<<kOCBlocks, 256, 0, s>>>(N, x, w.f0, w.bounds, move, exponent, floor_, xnew);
-    k_cone<<<kOCBlocks, 256, 0, s>>>(n, offsets, weights, count, xnew, w.f2, w.bounds);
+    k_cone_filter<<<cone_grid(n), kConeBlock, 0, s>>>(n, offsets, weights, count, xnew, w.f2, w.bounds);
     k_paper_volume<<<kOCBlocks, 256, 0, s>>>(N, w.f2, hs, beta, eta, emin, volume, w.bounds, w.partials, w.ticket);
   }
   k_absmax_diff<<<1, 1024, 0, s>>>(N, xnew, x, w.bounds + 4);

@@ -485,6 +485,21 @@ def test_paper_chain_matches_oracle(pkg, oracle):
     assert po.change.shape == (1,) and int(po.bounds[3]) == steps and not bool(po.bounds[2])
 
 
+@pytest.mark.parametrize("n,rmin", [(37, 2.1), (64, 3.0), (13, 5.5), (20, 7.0)])
+def test_cone_filter_matches_oracle(pkg, oracle, n, rmin):
+    """The clipped cone filter against the oracle: grids that end inside a 32 x 8 column tile, and
+    tap tables longer than one shared-memory chunk of 512 (rmin 5.5: 739 taps, 7.0: 1365)."""
+    rng = np.random.default_rng(n)
+    x = rng.uniform(0.0, 1.0, (n, n, n))
+    po = pkg.PaperOuter(n, 0.3, rmin=rmin)
+    out = torch.empty((n, n, n), device="cuda", dtype=torch.float64)
+    po.raw_filter(torch.tensor(x, device="cuda"), out)
+    assert rel(out.cpu().numpy(), oracle.cone_filter(x, rmin)) < 1e-13
+    again = torch.empty_like(out)
+    po.raw_filter(torch.tensor(x, device="cuda"), again)
+    assert torch.equal(out, again)
+
+
 def test_design_step_objective_and_sensitivity(pkg, oracle):
     """One Study II design step: solve, shear objective / local energy, OC update (verify.py:39-96)."""
     n = 8
